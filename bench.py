@@ -1,0 +1,527 @@
+#!/usr/bin/env python3
+"""Throughput of one sub-iteration of XPRecon's iterative cone-beam path on B200.
+
+Metric (the reference's headline): GUPS = voxels x projections-per-sub-iteration
+/ sub-iteration time / 1e9, a sub-iteration being forward projection + error +
+multiplicative back-projection (reconstruction_n.hpp:65-76) over one angular
+subset.  Workload: the 512^3-phantom configuration -- the reference derives a
+768^3 reconstruction grid from the 768 x 768 detector (geometry.hpp:50-56);
+720 projections over 360 degrees, sit = 10, so 72 projections per sub-iteration;
+px 0.1 mm, so 100, sd 1000, rx 1.5 px, sx -2, sy 3 (mm).  Data are synthetic
+(seeded ellipsoid phantom + textured background, projected with this library's
+forward projector, Poisson noise at 1e5 photons, -log preprocessing on the GPU).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--arith fast|strict] [--storage fp32|bf16|fp16] [--config c2|c1]
+
+Under torchrun each rank reconstructs its own volume (weak scaling, no
+collective on the data path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "c2": dict(desc="768^3 recon grid (512^3 phantom: 40 ellipsoids + 5% textured background), "
+                    "720 projections of 768x768, sit=10 -> 72 per sub-iteration",
+               dwidth=768, dheight=768, projections=720, sit=10, px=0.1, so=100.0, sd=1000.0, rx=1.5, sx=-2.0,
+               sy=3.0, phantom=512, ellipsoids=40, background=0.05, i0=1e5, seed=2),
+    "c1": dict(desc="192^3 recon grid (128^3 phantom: 10 ellipsoids), 180 projections of 192x192, sit=10 -> 18",
+               dwidth=192, dheight=192, projections=180, sit=10, px=0.1, so=100.0, sd=1000.0, rx=0.0, sx=0.0,
+               sy=0.0, phantom=128, ellipsoids=10, background=0.0, i0=1e5, seed=1),
+}
+
+FLOPS_PER_PAIR = 44          # algorithmic FP32 operations per (voxel, projection) pair, forward + backward
+NOMINAL_FP32_LANES = 148 * 128
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--arith", choices=["fast", "strict"], default="fast")
+    p.add_argument("--storage", choices=["fp32", "bf16", "fp16"], default="fp32")
+    p.add_argument("--config", choices=sorted(CONFIGS), default="c2")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def emit(obj):
+    print(json.dumps(obj), flush=True)
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % os.getpid())
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for i, n in enumerate(names):
+                if r[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- synthetic data
+def make_phantom(cfg, vx, W, Hv, device, seed):
+    """Seeded ellipsoid phantom (+ smooth Gaussian-textured background) in the central
+    phantom^3 region of the (y, z, x) grid; values are attenuation per voxel (mu * vx)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    vol = torch.zeros((Hv, W, W), dtype=torch.float32, device=device)
+    ph = cfg["phantom"]
+    c0 = np.array([W / 2.0, Hv / 2.0, W / 2.0])  # x, y, z centre in voxels
+    mus = []
+    for _ in range(cfg["ellipsoids"]):
+        while True:
+            cx, cz = rng.uniform(-ph / 2, ph / 2, 2)
+            if cx * cx + cz * cz <= (ph / 2) ** 2:
+                break
+        cy = rng.uniform(-ph / 2, ph / 2)
+        axes = rng.uniform(0.03, 0.25, 3) * ph
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        mu = rng.uniform(0.0, 0.02)
+        mus.append(mu)
+        cen = c0 + np.array([cx, cy, cz])
+        r = axes.max()
+        lo = np.maximum(np.floor(cen - r).astype(int), 0)
+        hi = np.minimum(np.ceil(cen + r).astype(int) + 1, [W, Hv, W])
+        if (hi <= lo).any():
+            continue
+        xs = torch.arange(lo[0], hi[0], device=device, dtype=torch.float32) - float(cen[0])
+        ys = torch.arange(lo[1], hi[1], device=device, dtype=torch.float32) - float(cen[1])
+        zs = torch.arange(lo[2], hi[2], device=device, dtype=torch.float32) - float(cen[2])
+        Y, Z, X = torch.meshgrid(ys, zs, xs, indexing="ij")
+        P = torch.stack([X, Y, Z], dim=-1) @ torch.from_numpy(q.astype(np.float32)).to(device)
+        inside = ((P / torch.from_numpy(axes.astype(np.float32)).to(device)) ** 2).sum(-1) <= 1.0
+        vol[lo[1]:hi[1], lo[2]:hi[2], lo[0]:hi[0]] += inside.float() * float(mu * vx)
+        del Y, Z, X, P, inside
+    if cfg["background"] > 0:
+        g = torch.Generator(device=device).manual_seed(seed)
+        noise = torch.randn((1, 1, ph, ph, ph), device=device, generator=g)
+        k = torch.exp(-0.5 * (torch.arange(-12, 13, device=device, dtype=torch.float32) / 4.0) ** 2)
+        k = k / k.sum()
+        import torch.nn.functional as F
+        noise = F.conv3d(noise, k.view(1, 1, -1, 1, 1), padding=(12, 0, 0))
+        noise = F.conv3d(noise, k.view(1, 1, 1, -1, 1), padding=(0, 12, 0))
+        noise = F.conv3d(noise, k.view(1, 1, 1, 1, -1), padding=(0, 0, 12))[0, 0]
+        noise = noise / noise.std()
+        level = cfg["background"] * float(np.mean(mus)) * vx
+        bg = torch.clamp(level * (1.0 + noise), min=0.0)
+        y0, x0 = (Hv - ph) // 2, (W - ph) // 2
+        vol[y0:y0 + ph, x0:x0 + ph, x0:x0 + ph] += bg
+        del noise, bg
+    return vol.reshape(-1).contiguous()
+
+
+class Problem:
+    """Device-resident state of one reconstruction of the benchmark configuration."""
+
+    def __init__(self, cfg, arith, storage, device_index, seed):
+        import torch
+        from xpulse_recon_b200 import _lib
+        from xpulse_recon_b200.projector import Context, JitterSource, geometry
+        self.torch, self.L = torch, _lib.lib()
+        self.cfg = cfg
+        self.arith = _lib.FAST if arith == "fast" else _lib.STRICT
+        self.storage = {"fp32": _lib.F32, "bf16": _lib.BF16, "fp16": _lib.F16}[storage]
+        self.tdt = {"fp32": torch.float32, "bf16": torch.bfloat16, "fp16": torch.float16}[storage]
+        self.ctx = Context(device_index)
+        self.device = torch.device("cuda", device_index)
+        kw = {k: cfg[k] for k in ("dwidth", "dheight", "projections", "sit", "px", "so", "sd", "rx", "sx", "sy")}
+        self.pd_all, self.g = geometry(**kw)
+        self.P, self.S = cfg["projections"], cfg["sit"]
+        self.Pc, self.W, self.Hv = self.g["concurrent"], self.g["vwidth"], self.g["vheight"]
+        self.Wd, self.Hd = cfg["dwidth"], cfg["dheight"]
+        self.nvox = self.W * self.Hv * self.W
+        self.npix = self.Pc * self.Wd * self.Hd
+        self.jitter = JitterSource(seed)
+        self.stream = torch.cuda.Stream(device=self.device)
+        self.sp = C.c_void_p(self.stream.cuda_stream)
+        d = self.device
+        self.pd_sub = []
+        for s in range(self.S):
+            idx = [s + k * self.S for k in range(self.Pc)]
+            self.pd_sub.append(torch.from_numpy(np.ascontiguousarray(self.pd_all[idx])).to(d))
+        # measured projections: simulate with the forward projector, Poisson noise, -log on the GPU
+        with torch.cuda.stream(self.stream):
+            phantom = make_phantom(cfg, self.g["vx"], self.W, self.Hv, d, seed)
+            self.images = []
+            sums = torch.zeros(self.npix, dtype=torch.int32, device=d)
+            gen = torch.Generator(device=d).manual_seed(seed + 1)
+            for s in range(self.S):
+                sums.zero_()
+                self._forward(phantom, sums, s, list(self.g["orig"]))
+                p = sums.view(torch.int32).to(torch.int64).bitwise_and(0xFFFFFFFF).to(torch.float32) / float(1 << 22)
+                inten = torch.poisson(cfg["i0"] * torch.exp(-p), generator=gen) / cfg["i0"]
+                out = torch.empty(self.npix, dtype=self.tdt, device=d)
+                _lib.check(self.L.xpr_preprocess_apply(self.ctx.handle, inten.data_ptr(), out.data_ptr(), self.storage,
+                                                       self.npix, 0, None, 1, self.sp), "preprocess")
+                self.images.append(out)
+                del p, inten
+            self.phantom_host = None
+            self.phantom = phantom
+            self.vol = torch.ones(self.nvox, dtype=torch.float32, device=d)
+            self.sums = torch.full((self.npix,), 1 << 22, dtype=torch.int32, device=d)
+            self.ratio = self.sums if self.storage == _lib.F32 else torch.empty(self.npix, dtype=self.tdt, device=d)
+            self.residual = torch.zeros(1, dtype=torch.float64, device=d)
+        self.stream.synchronize()
+        self.sit_next = 0
+        self.weight = 1.0
+        # the first sub-iteration has no forward (reconstruction_n.hpp:70): run it untimed
+        self.subiteration(first=True)
+        self.stream.synchronize()
+
+    def launch_desc(self, origin):
+        from xpulse_recon_b200 import _lib
+        L = _lib.Launch()
+        L.vmin[:] = [0, 0, 0]
+        L.vmax[:] = [self.W, self.Hv, self.W]
+        L.origin[:] = origin
+        L.voxel[:] = [self.g["vx"]] * 3
+        L.det_w, L.rows, L.row_offset = self.Wd, self.Hd, 0
+        L.n_angles, L.modules = self.Pc, 1
+        L.arith = self.arith
+        return L
+
+    def _forward(self, vol, sums, s, origin):
+        from xpulse_recon_b200 import _lib
+        L = self.launch_desc(origin)
+        _lib.check(self.L.xpr_forward(self.ctx.handle, vol.data_ptr(), sums.data_ptr(), self.pd_sub[s].data_ptr(),
+                                      self.Pc, C.byref(L), self.sp), "forward")
+
+    def next_origin(self):
+        o = []
+        for i in range(3):
+            o.append(float(np.float32(np.float32(self.g["orig"][i]) + np.float32(self.jitter.draw(self.g["vx"])))))
+        return o
+
+    def subiteration(self, first=False, events=None, images=None):
+        """forward -> error -> backward -> reset sums, with optional per-kernel events."""
+        from xpulse_recon_b200 import _lib
+        s = self.sit_next
+        self.sit_next = (s + 1) % self.S
+        L = self.launch_desc(self.next_origin())
+        h, sp = self.ctx.handle, self.sp
+        img = self.images[s] if images is None else images
+        if events:
+            events[0].record(self.stream)
+        if not first:
+            _lib.check(self.L.xpr_forward(h, self.vol.data_ptr(), self.sums.data_ptr(), self.pd_sub[s].data_ptr(),
+                                          self.Pc, C.byref(L), sp), "forward")
+        if events:
+            events[1].record(self.stream)
+        _lib.check(self.L.xpr_error(h, img.data_ptr(), self.storage, self.sums.data_ptr(), self.ratio.data_ptr(),
+                                    self.storage, self.npix, self.weight, _lib.ERROR_STD, 1,
+                                    self.residual.data_ptr(), sp), "error")
+        if events:
+            events[2].record(self.stream)
+        _lib.check(self.L.xpr_backward(h, self.vol.data_ptr(), self.ratio.data_ptr(), self.storage,
+                                       self.pd_sub[s].data_ptr(), self.Pc, C.byref(L), sp), "backward")
+        if events:
+            events[3].record(self.stream)
+        if self.ratio is self.sums:  # in-place FP32 ratio: reset the sums for the next forward
+            _lib.check(self.L.xpr_fill_u32(h, self.sums.data_ptr(), 0, self.npix, sp), "fill")
+        return s
+
+
+# ----------------------------------------------------------------------------- CPU (reference kernels)
+def cpu_reference_step_factory(cfg, seconds_target):
+    """The reference's own OpenCL kernels (oracle/_ref, built from its sources) on the host
+    cores: forward + error + backward of a y-slab of the grid against one sub-iteration's
+    72 projections.  Returns (step_fn, info)."""
+    from oracle import oracle as O
+    R = O.ref_lib()
+    kind = "reference"
+    if R is None:
+        kind = "port"
+    gp = O.geom_params(**{k: cfg[k] for k in ("dwidth", "dheight", "projections", "sit", "px", "so", "sd", "rx",
+                                               "sx", "sy")})
+    pd_all, go = O.geometry(gp)
+    Pc, W, Hv, Wd, Hd = int(go.concurrent), int(go.vwidth), int(go.vheight), cfg["dwidth"], cfg["dheight"]
+    pd = O.subset_projdata(pd_all, cfg["projections"], cfg["sit"], 1, 1, Pc)
+    rng = np.random.default_rng(9)
+    images = rng.uniform(0.02, 0.3, Pc * Wd * Hd).astype(np.float32)
+    origin = [float(np.float32(go.orig[i]) + np.float32(0.37 * go.vx)) for i in range(3)]
+    y_mid = Hv // 2
+
+    def run(layers):
+        y0 = y_mid - layers // 2
+        n = W * layers * W
+        vol = rng.uniform(1e-4, 3e-4, O.ndrange(n)).astype(np.float32)
+        sums = np.zeros(Pc * Wd * Hd, np.uint32)
+        t = time.perf_counter()
+        if kind == "reference":
+            O.ref_forward(vol, sums, pd, Wd, Hd, origin, Pc, 1, (0, y0, 0), (W, y0 + layers, W), (0, Hd),
+                          [go.vx] * 3)
+            O.ref_error(images, sums, Wd, Hd, 1.0)
+            O.ref_backward(vol, sums.view(np.float32), pd, Wd, Hd, origin, Pc, 1, (0, y0, 0), (W, y0 + layers, W),
+                           (0, Hd), [go.vx] * 3)
+        else:
+            L, keep = O.make_launch((0, y0, 0), (W, y0 + layers, W), origin, [go.vx] * 3, Wd, Hd, 0, Pc, 1)
+            O.forward(vol, sums, pd, L)
+            O.error(images, sums, 1.0)
+            O.backward(vol, sums.view(np.float32), pd, L)
+        return time.perf_counter() - t, n * Pc
+
+    dt, pairs = run(1)
+    layers = int(max(1, min(Hv, round(seconds_target / max(dt, 1e-3)))))
+    info = {"kind": kind, "cores": os.cpu_count(), "layers": layers, "W": W, "Pc": Pc}
+    return (lambda: run(layers)), info
+
+
+def cpu_baseline(cfg, seconds):
+    step, info = cpu_reference_step_factory(cfg, seconds)
+    dt, pairs = step()
+    return {"value": pairs / dt / 1e9, "unit": "GUPS", "cores": info["cores"], "kind": info["kind"],
+            "sample": "forward + error + backward of a %d-layer y-slab (%dx%dx%d voxels) against one "
+                      "sub-iteration's %d projections, OpenMP on %d host threads, %.1f s"
+                      % (info["layers"], info["W"], info["layers"], info["W"], info["Pc"], info["cores"], dt)}
+
+
+# ----------------------------------------------------------------------------- main arms
+def run_reference(args, cfg, rank, world):
+    if rank != 0:
+        return 0
+    step, info = cpu_reference_step_factory(cfg, max(1.0, min(10.0, 60.0 / max(1, args.steps + args.warmup))))
+    for _ in range(args.warmup):
+        step()
+    tot_t, tot_p = 0.0, 0
+    for _ in range(args.steps):
+        dt, p = step()
+        tot_t += dt
+        tot_p += p
+    v = tot_p / tot_t / 1e9
+    sample = ("forward + error + backward of a %d-layer y-slab of the %d^3 grid against %d projections per step"
+              % (info["layers"], info["W"], info["Pc"]))
+    emit({"impl": "reference", "metric": "GUPS per sub-iteration (voxel x projection pairs / s)", "value": v,
+          "unit": "GUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+          "ms_per_step": 1000.0 * tot_t / args.steps, "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+          "config": {"workload": args.config + ": " + cfg["desc"], "arith": "reference OpenCL kernels, IEEE fp32",
+                     "storage": "fp32"},
+          "cpu_baseline": {"value": v, "unit": "GUPS", "cores": info["cores"], "kind": info["kind"],
+                           "sample": sample},
+          "e2e": {"value": v, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    return 0
+
+
+def run_ours(args, cfg, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    prob = Problem(cfg, args.arith, args.storage, local, cfg["seed"] + 1000 * rank)
+    stream = prob.stream
+    K, Wm = args.steps, args.warmup
+    for _ in range(Wm):
+        prob.subiteration()
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    for k in range(K):
+        prob.subiteration(events=evs[k])
+    stream.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = evs[0][0].elapsed_time(evs[K - 1][3])
+    fwd = [e[0].elapsed_time(e[1]) for e in evs]
+    err = [e[1].elapsed_time(e[2]) for e in evs]
+    bwd = [e[2].elapsed_time(e[3]) for e in evs]
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    pairs_step = prob.nvox * prob.Pc
+    value = pairs_step * K * world / (total_ms / 1000.0) / 1e9
+
+    # ---- e2e: host buffers through the C ABI; uploads overlapped on a copy stream
+    from xpulse_recon_b200 import _lib
+    L = prob.L
+    nbytes = prob.npix * prob.images[0].element_size()
+    pinned = []
+    for s in range(prob.S):
+        hp = C.c_void_p()
+        _lib.check(L.xpr_alloc_pinned(prob.ctx.handle, nbytes, C.byref(hp)), "alloc_pinned")
+        C.memmove(hp, prob.images[s].cpu().numpy().ctypes.data, nbytes)
+        pinned.append(hp)
+    res_host = C.c_void_p()
+    _lib.check(L.xpr_alloc_pinned(prob.ctx.handle, 8, C.byref(res_host)), "alloc_pinned")
+    dbuf = [torch.empty_like(prob.images[0]) for _ in range(2)]
+    copy_stream = torch.cuda.Stream(device=prob.device)
+    cs = C.c_void_p(copy_stream.cuda_stream)
+    up_done = [torch.cuda.Event() for _ in range(2)]
+    used = [torch.cuda.Event() for _ in range(2)]
+
+    def e2e_steps(n, timed):
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        start.record(prob.stream)
+        s0 = prob.sit_next
+        _lib.check(L.xpr_upload(prob.ctx.handle, dbuf[0].data_ptr(), pinned[s0], nbytes, cs), "upload")
+        up_done[0].record(copy_stream)
+        for k in range(n):
+            b = k % 2
+            if k + 1 < n:  # prefetch the next subset while this one computes
+                nb = (k + 1) % 2
+                if k >= 1:
+                    copy_stream.wait_event(used[nb])
+                nxt = (prob.sit_next + 1) % prob.S
+                _lib.check(L.xpr_upload(prob.ctx.handle, dbuf[nb].data_ptr(), pinned[nxt], nbytes, cs), "upload")
+                up_done[nb].record(copy_stream)
+            prob.stream.wait_event(up_done[b])
+            prob.subiteration(images=dbuf[b])
+            used[b].record(prob.stream)
+            _lib.check(L.xpr_download(prob.ctx.handle, res_host, prob.residual.data_ptr(), 8, prob.sp), "download")
+        end.record(prob.stream)
+        prob.stream.synchronize()
+        return start.elapsed_time(end)
+
+    e2e_steps(min(2, K), False)
+    e2e_ms = e2e_steps(K, True)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = pairs_step * K * world / (e2e_ms / 1000.0) / 1e9
+    for hp in pinned:
+        L.xpr_free_pinned(prob.ctx.handle, hp)
+    L.xpr_free_pinned(prob.ctx.handle, res_host)
+
+    # ---- roofline of the dominant kernel
+    f_ms, b_ms = statistics.mean(fwd), statistics.mean(bwd)
+    dom = "backward" if b_ms >= f_ms else "forward"
+    dom_ms = max(f_ms, b_ms)
+    isz = prob.images[0].element_size()
+    if dom == "forward":
+        alg_bytes = 4 * prob.nvox + 4 * prob.npix
+    else:
+        alg_bytes = 8 * prob.nvox + isz * prob.npix
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / (dom_ms / 1000.0) / 1e9
+    sm_mhz = (clk or {}).get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = NOMINAL_FP32_LANES * 2 * float(sm_mhz) * 1e6 / 1e12
+    step_ms = total_ms / K
+    line = {
+        "metric": "GUPS per sub-iteration (voxel x projection pairs / s)",
+        "value": value, "unit": "GUPS", "n_gpus": world, "steps": K, "warmup": Wm,
+        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.config + ": " + cfg["desc"], "grid": [prob.W, prob.Hv, prob.W],
+                   "projections": prob.P, "sit": prob.S, "per_subiteration": prob.Pc, "arith": args.arith,
+                   "storage": args.storage, "l2": "inputs larger than L2 (%.2f GB volume, %.0f MB subset)"
+                   % (4 * prob.nvox / 1e9, isz * prob.npix / 1e6), "parallelism": "independent volume per rank"},
+        "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": 8},
+        "gpu_launches": 3 * K,
+        "kernels_ms": {"forward": f_ms, "error": statistics.mean(err), "backward": b_ms},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "note": "issue/atomic-bound (not a dense contraction, not HBM-bound): see compute"},
+        "compute": {"flops_per_pair": FLOPS_PER_PAIR, "achieved_tflops": FLOPS_PER_PAIR * pairs_step / (step_ms / 1000) / 1e12,
+                    "peak_fp32_tflops": fp32_peak, "frac": FLOPS_PER_PAIR * pairs_step / (step_ms / 1000) / 1e12 / fp32_peak,
+                    "peak_source": "nominal: 148 SM x 128 FP32 lanes x 2 x median SM clock"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(cfg, args.cpu_seconds)
+        except Exception as e:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    if rank == 0:
+        emit(line)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    cfg = CONFIGS[args.config]
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, cfg, rank, world)
+    return run_ours(args, cfg, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,186 @@
+/*
+ * xpr.h -- C ABI of the B200 backend for the XPRecon iterative cone-beam path.
+ *
+ * The reference (ebarjou/xpulse_recon) has no library boundary: its operator
+ * seam is the protected API of class Reconstruction (src/reconstruction.hpp:
+ * 166-312) driving five OpenCL kernels through gpu::Context / gpu::Kernel
+ * (src/reconstruction/gpu/context.hpp, kernel.hpp).  This header is the plain-C
+ * replacement for that seam: plain pointers and sizes, status codes instead of
+ * exceptions, explicit streams instead of the three in-order OpenCL queues.
+ *
+ * Conventions
+ *   - Every function returns XPR_OK (0) or a positive XPR_ERR_* code; the
+ *     message of the last failure on the calling thread is xpr_last_error().
+ *   - "device" pointers are CUDA device memory of the context's GPU; "host"
+ *     pointers are ordinary or pinned host memory.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ *     Operator calls are asynchronous with respect to the host.
+ *   - Volumes are laid out (y, z, x) with x fastest: index = (y*Z + z)*X + x,
+ *     the layout of utils.cl:39-45 (to3D).  Detector images are (image, row,
+ *     column): index = img*(W*rows) + v*W + u (utils.cl:47).
+ *   - Forward sums are 22-bit-fraction unsigned fixed point (constants.cl:17-23),
+ *     accumulated modulo 2^32.
+ */
+#ifndef XPR_H
+#define XPR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XPR_ABI_VERSION 1
+
+enum xpr_status {
+    XPR_OK = 0,
+    XPR_ERR_INVALID = 1,     /* bad argument */
+    XPR_ERR_CUDA = 2,        /* CUDA runtime error */
+    XPR_ERR_OOM = 3,         /* device or pinned allocation failed */
+    XPR_ERR_CAP = 4,         /* request exceeds the context's device-memory cap */
+    XPR_ERR_IO = 5,          /* file read / write failure */
+    XPR_ERR_PARAM = 6,       /* malformed or inconsistent parameters (JSON, geometry) */
+    XPR_ERR_UNSUPPORTED = 7  /* valid request this build does not implement */
+};
+
+enum xpr_arith { XPR_ARITH_STRICT = 0, XPR_ARITH_FAST = 1 };
+enum xpr_dtype { XPR_F32 = 0, XPR_BF16 = 1, XPR_F16 = 2 };
+enum xpr_error_mode {
+    XPR_ERROR_STD = 0,       /* KernelError.cl:8-24: log(max(ref/max(got,eps),eps))*w */
+    XPR_ERROR_FIRST_1C = 1,  /* reconstruction_lplh.hpp:164-177: log(max(ref,eps)) */
+    XPR_ERROR_1C = 2         /* reconstruction_lplh.hpp:140-163 (std::max semantics) */
+};
+
+/* ProjData (constants.cl:25-28): the 4 columns of the glm projection matrix,
+ * then the viewport {l, r, b, t}.  80 bytes, the reference's layout.
+ * Viewport bounds must be integers in [0, 2^22]. */
+typedef struct xpr_projdata {
+    float mvp[16];
+    float vp[4];
+} xpr_projdata;
+
+/* One projector launch: the scalar arguments of Forward/Backward
+ * (constants.cl:30-54, set by reconstruction.hpp:208-281) and the index lists
+ * of ForwardH/BackwardH (constants.cl:62-88). */
+typedef struct xpr_launch {
+    int32_t vmin[3];          /* voxel box [vmin, vmax) in (x, y, z) (setVolumeParameters) */
+    int32_t vmax[3];
+    float origin[3];          /* volume origin in mm incl. jitter (setOrigin) */
+    float voxel[3];           /* voxel size in mm */
+    uint32_t det_w;           /* detector width (setImageParameters: size.x) */
+    uint32_t rows;            /* rows held per image in the buffer (setImageOffset: y) */
+    int32_t row_offset;       /* first detector row held (setImageOffset: x) */
+    uint32_t n_angles;        /* angles in the subset (setAngleNumber) */
+    uint32_t modules;         /* modules per angle */
+    const uint16_t *list_mvp; /* optional device list: ProjData index per entry (ForwardH) */
+    const uint16_t *list_img; /* optional device list: image slot per entry */
+    uint32_t n_list;
+    int32_t arith;            /* xpr_arith */
+    int32_t compat_pad;       /* also run the reference NDRange padding work-items (kernel.hpp:73-81);
+                                 the volume buffer must then hold xpr_ndrange(n) floats */
+    int32_t nan_skip;         /* BackwardH: NaN ratios are skipped (KernelBackwardH.cl:36) */
+} xpr_launch;
+
+typedef struct xpr_ctx xpr_ctx;
+
+/* ---------------------------------------------------------------- context */
+/* Replaces gpu::Context() (context.hpp:36-113).  mem_cap_bytes = 0: no cap
+ * beyond what cudaMemGetInfo reports (the reference's VRAM-filling probe,
+ * context.hpp:90-104, is not reproduced). */
+int xpr_create(int device, uint64_t mem_cap_bytes, xpr_ctx **out);
+int xpr_destroy(xpr_ctx *ctx);
+const char *xpr_last_error(void);
+int xpr_abi_version(void);
+/* usable device bytes: min(free memory, cap - bytes allocated through the context) */
+int xpr_mem_available(xpr_ctx *ctx, uint64_t *bytes);
+/* work-items of the reference NDRange for n items: n + (32 - n % 32) (kernel.hpp:73-81) */
+uint64_t xpr_ndrange(uint64_t n);
+
+/* ---------------------------------------------------------------- memory */
+/* Replace Context::createBuffer / setBuffer / getBuffer (context.hpp:152-300). */
+int xpr_alloc(xpr_ctx *ctx, uint64_t bytes, void **dptr);
+int xpr_free(xpr_ctx *ctx, void *dptr);
+int xpr_alloc_pinned(xpr_ctx *ctx, uint64_t bytes, void **hptr);
+int xpr_free_pinned(xpr_ctx *ctx, void *hptr);
+int xpr_upload(xpr_ctx *ctx, void *dst, const void *src, uint64_t bytes, void *stream);
+int xpr_download(xpr_ctx *ctx, void *dst, const void *src, uint64_t bytes, void *stream);
+/* fill `count` 32-bit words (enqueueFillBuffer; 1.0f is 0x3f800000) */
+int xpr_fill_u32(xpr_ctx *ctx, void *dst, uint32_t value, uint64_t count, void *stream);
+int xpr_synchronize(xpr_ctx *ctx, void *stream);
+
+/* ---------------------------------------------------------------- operators */
+/* Forward projection (Reconstruction::forward, reconstruction.hpp:294-296;
+ * KernelForward.cl:10-55, KernelForwardH.cl:8-37 when L->list_mvp is set):
+ * sum[img][v][u] += fixed(vol[voxel]) for every in-bounds (voxel, ProjData) pair.
+ * pd: n_pd device ProjData; without a list, entries 0 .. n_angles*modules-1 are
+ * used and image slot = entry / modules. */
+int xpr_forward(xpr_ctx *ctx, const float *vol, uint32_t *sum, const xpr_projdata *pd, uint32_t n_pd,
+                const xpr_launch *L, void *stream);
+
+/* Back projection with the multiplicative update (Reconstruction::backward,
+ * reconstruction.hpp:310-312; KernelBackward.cl:8-40, KernelBackwardH.cl:8-42):
+ * vol *= exp(sum of in-bounds ratios / their count).  ratio has ratio_dtype. */
+int xpr_backward(xpr_ctx *ctx, float *vol, const void *ratio, int ratio_dtype, const xpr_projdata *pd,
+                 uint32_t n_pd, const xpr_launch *L, void *stream);
+
+/* Error step (Reconstruction::error, reconstruction.hpp:302-304; KernelError.cl:8-24).
+ * images: n measured values of image_dtype.  sum: n fixed-point sums.  ratio:
+ * output of ratio_dtype; ratio == sum with XPR_F32 writes in place as the
+ * reference does.  When zero_sum != 0 (and ratio != sum) the sums are reset to 0
+ * in the same pass.  residual: optional device double, += sum of ratio^2 (FP64). */
+int xpr_error(xpr_ctx *ctx, const void *images, int image_dtype, uint32_t *sum, void *ratio, int ratio_dtype,
+              uint64_t n, float weight, int mode, int zero_sum, double *residual, void *stream);
+
+/* -log / normalise preprocessing (data_loader.hpp:48-101) on the device.
+ * minmax: device float[2] running {min, max} of the std::isnormal values,
+ * initialise to {FLT_MAX, FLT_MIN} as data_loader.hpp:12-13 does. */
+int xpr_preprocess_minmax(xpr_ctx *ctx, const float *images, uint64_t n, float *minmax, void *stream);
+/* v = normalize ? (isnormal(v) ? (v-min)/(max-min) : (max+min)/2) : v;
+ * v = mlog ? -log(clamp(v, eps, 1-eps)) : v; written as out_dtype into out
+ * (out may equal images for XPR_F32). */
+int xpr_preprocess_apply(xpr_ctx *ctx, const float *images, void *out, int out_dtype, uint64_t n, int normalize,
+                         const float *minmax, int mlog, void *stream);
+
+/* One sub-iteration of reconstruction_n.hpp:65-76: [forward] -> error -> backward,
+ * then the sums reset to 0.  first != 0 skips the forward (the sums must then
+ * hold FIXED_ONE, as after reconstruction_n.hpp:60).  ratio may equal sum (FP32
+ * in place) or be a separate buffer of ratio_dtype. */
+int xpr_subiteration(xpr_ctx *ctx, float *vol, uint32_t *sum, const void *images, int image_dtype, void *ratio,
+                     int ratio_dtype, const xpr_projdata *pd, uint32_t n_pd, const xpr_launch *L, float weight,
+                     int first, double *residual, void *stream);
+
+/* ---------------------------------------------------------------- geometry (host) */
+/* Geometry parameters (global_parameters.hpp:23-54, parameters.hpp:34-48). */
+typedef struct xpr_geom_params {
+    float so, sd, angle, heli_offset;
+    float px, rx_px, sx, sy;            /* rx in pixels as in the JSON; sx, sy act in mm (geometry.hpp:61) */
+    int64_t module_number;
+    int32_t module_angle_offset_set;
+    float module_angle_offset;
+    float module_center_offset_z;
+    int64_t dwidth, dheight, projections, sit;
+    const float *angle_list;            /* optional, `projections` angles in degrees */
+    const float *mod_offset;            /* optional extension: 3 per module, pixels */
+    const float *mod_rpy;               /* optional extension: roll, pitch, yaw per module, degrees */
+} xpr_geom_params;
+
+typedef struct xpr_geom_out {
+    float vx;
+    int64_t vwidth, vheight;
+    float orig[3];
+    int64_t concurrent;                 /* floor(projections / sit) */
+} xpr_geom_out;
+
+/* Geometry() + computeMVPs() (geometry.hpp:35-76, 182-328): ProjData for every
+ * (angle, module) in angle-major order (index angle*modules + module).
+ * fp64 != 0 builds the matrices in double precision. */
+int xpr_geometry(const xpr_geom_params *gp, int fp64, xpr_projdata *out, xpr_geom_out *go);
+
+/* The origin jitter sequence: n draws of std::uniform_real_distribution<float>(0, vx)
+ * from std::mt19937(seed) (reconstruction.hpp:268-272), 3 per sub-iteration. */
+int xpr_jitter(uint32_t seed, uint64_t n, float vx, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,245 @@
+"""Pins of the CPU oracle (no GPU).
+
+The reference ships no tests, fixtures or golden vectors for this path, so the
+oracle's restatement is pinned against (a) the reference's own OpenCL kernel
+sources compiled for the CPU (oracle/_ref) -- bit for bit -- and (b) known-answer
+tests derived from the geometry and the fixed-point format.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.cases import CASES, make_case, oracle_backward, oracle_forward, ratio_from
+
+
+# ----------------------------------------------------------------------------- reference kernels
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_forward_matches_reference_kernel(ref, name):
+    c = make_case(name, sit=1, seed=1)
+    sums_ref = np.zeros(c["Pc"] * c["Wd"] * c["rows"], np.uint32)
+    O.ref_forward(c["vol"], sums_ref, c["pd"], c["Wd"], c["Hd"], c["origin"], c["Pc"], c["M"], c["vmin"],
+                  c["vmax"], (0, c["rows"]), [c["go"].vx] * 3)
+    sums = oracle_forward(c, O.STRICT, compat_pad=1)
+    assert sums_ref.sum(dtype=np.uint64) > 0
+    np.testing.assert_array_equal(sums, sums_ref)
+
+
+@pytest.mark.parametrize("name", ["plain48", "offsets64", "modules2", "ragged"])
+def test_forward_row_window_matches_reference_kernel(ref, name):
+    """method_2's cropped detector window (lineOffsetY = {iOffset, iSize}); rows reach the
+    detector bottom so the reference's unclipped bound (H14) never overflows."""
+    base = make_case(name)
+    off = base["Hd"] // 3
+    c = make_case(name, sit=1, seed=2, row_window=(off, base["Hd"] - off),
+                  box=((0, 2, 0), (base["W"], base["go"].vheight - 1, base["W"])))
+    sums_ref = np.zeros(c["Pc"] * c["Wd"] * c["rows"], np.uint32)
+    O.ref_forward(c["vol"], sums_ref, c["pd"], c["Wd"], c["Hd"], c["origin"], c["Pc"], c["M"], c["vmin"],
+                  c["vmax"], (off, c["rows"]), [c["go"].vx] * 3)
+    np.testing.assert_array_equal(oracle_forward(c, O.STRICT, compat_pad=1), sums_ref)
+
+
+@pytest.mark.parametrize("name", ["plain48", "offsets64", "ragged", "modules3_rpy"])
+def test_error_and_backward_match_reference_kernel(ref, name):
+    c = make_case(name, sit=2, seed=3)
+    sums = oracle_forward(c, O.STRICT, compat_pad=1)
+    r_ref = sums.copy()
+    O.ref_error(c["images"][: sums.size], r_ref, c["Wd"], c["Hd"], 0.81)
+    r_orc = sums.copy()
+    O.error(c["images"][: sums.size], r_orc, 0.81)
+    np.testing.assert_array_equal(r_orc, r_ref)
+    ratio = r_ref.view(np.float32)
+    v_ref = c["vol"].copy()
+    O.ref_backward(v_ref, ratio, c["pd"], c["Wd"], c["Hd"], c["origin"], c["Pc"], c["M"], c["vmin"], c["vmax"],
+                   (0, c["rows"]), [c["go"].vx] * 3)
+    v_orc = oracle_backward(c, ratio, O.STRICT, compat_pad=1)
+    np.testing.assert_array_equal(v_orc.view(np.uint32), v_ref.view(np.uint32))
+    assert np.isnan(v_ref).any() and np.isfinite(v_ref).any()
+
+
+def test_forwardh_backwardh_match_reference_kernel(ref):
+    """KernelForwardH/BackwardH: one layer, culled angle list, NaN-skipping backward."""
+    c = make_case("offsets64", sit=1, seed=4)
+    gp, go = c["gp"], c["go"]
+    W = c["W"]
+    layer = 17
+    lm = np.zeros(64, np.uint16)
+    li = np.zeros(64, np.uint16)
+    n = O.lib().orc_cull_layer(O.C.byref(gp), O.C.byref(go), c["pd_all"], 1, layer, 0, lm, li)
+    lm, li = lm[:n].copy(), li[:n].copy()
+    assert 0 < n <= c["Pc"] + 1
+    vol = c["vol"][: O.ndrange(W * W)].copy()
+    origin4 = [*c["origin"], 1.0]
+    sums_ref = np.zeros((c["Pc"] + 1) * c["Wd"] * c["Hd"], np.uint32)
+    O.ref_lib().refk_forwardh(vol, sums_ref, c["pd_all"], lm, li, n, layer, (O.C.c_float * 4)(*origin4),
+                              go.vx, c["Wd"], c["Hd"], W, O.ndrange(W * W))
+    L, keep = O.make_launch((0, layer, 0), (W, layer + 1, W), c["origin"], [go.vx] * 3, c["Wd"], c["Hd"], 0,
+                            c["Pc"] + 1, 1, compat_pad=1, list_mvp=lm, list_img=li)
+    sums = np.zeros_like(sums_ref)
+    O.forward(vol, sums, c["pd_all"], L)
+    np.testing.assert_array_equal(sums, sums_ref)
+    ratio = c["images"][: sums.size].copy()
+    ratio[::7] = np.nan
+    v_ref = vol.copy()
+    O.ref_lib().refk_backwardh(v_ref, ratio, c["pd_all"], lm, li, n, layer, (O.C.c_float * 4)(*origin4),
+                               go.vx, c["Wd"], c["Hd"], W, O.ndrange(W * W))
+    L.nan_skip = 1
+    v = vol.copy()
+    O.backward(v, ratio, c["pd_all"], L)
+    np.testing.assert_array_equal(v.view(np.uint32), v_ref.view(np.uint32))
+
+
+# ----------------------------------------------------------------------------- known answers
+def test_mt19937_known_answer():
+    # the C++ standard fixes the 10000th output of a default-constructed mt19937 (seed 5489)
+    out = O.mt_outputs(5489, 10000)
+    assert int(out[-1]) == 4123659995
+
+
+def test_jitter_matches_libstdcxx(xlib):
+    """Oracle restatement == std::uniform_real_distribution<float> over std::mt19937 (product)."""
+    import ctypes as C
+    for seed in (0, 1, 5489, 123456789):
+        vx = np.float32(0.0130000003)
+        a = O.jitter_sequence(seed, 300, float(vx))
+        b = np.zeros(300, np.float32)
+        assert xlib.xpr_jitter(seed, 300, C.c_float(vx), b.ctypes.data) == 0
+        np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+        assert (a >= 0).all() and (a < vx).all()
+
+
+def _ulp_err(got, exact):
+    got = np.float64(got)
+    if math.isinf(exact) or exact == 0.0:
+        return 0.0 if got == exact else float("inf")
+    ulp = math.ldexp(1.0, math.frexp(exact)[1] - 24)
+    return abs(got - exact) / ulp
+
+
+def test_portable_exp_log_accuracy():
+    L = O.lib()
+    rng = np.random.default_rng(7)
+    xs = np.concatenate([rng.uniform(-87, 88, 4000), rng.uniform(-1, 1, 4000), rng.uniform(-20, 20, 2000),
+                         [0.0, -0.0, 1e-30, -1e-30, 88.72283, -87.3, -100.0, -103.9]]).astype(np.float32)
+    worst = max(_ulp_err(L.orc_expf(float(x)), math.exp(float(x))) for x in xs if math.exp(float(x)) > 1.2e-38)
+    assert worst <= 2.0, worst
+    ys = np.concatenate([10 ** rng.uniform(-37, 38, 4000), rng.uniform(0.5, 2.0, 4000),
+                         1 + rng.uniform(-1e-3, 1e-3, 2000), [1.0, 2.0, 0.5, 1e-40, 3e-45]]).astype(np.float32)
+    ys = ys[ys > 0]
+    worst = max(_ulp_err(L.orc_logf(float(y)), math.log(float(y))) for y in ys)
+    assert worst <= 2.5, worst
+    assert math.isnan(L.orc_expf(float("nan"))) and math.isnan(L.orc_logf(-1.0))
+    assert L.orc_logf(0.0) == -math.inf and L.orc_expf(100.0) == math.inf and L.orc_expf(-200.0) == 0.0
+
+
+def test_fixed_point_known_answers():
+    L = O.lib()
+    assert L.orc_float_to_fixed(1.0) == 1 << 22
+    assert L.orc_float_to_fixed(0.5) == 1 << 21
+    assert L.orc_float_to_fixed(float(np.float32(1.0) / np.float32(3.0))) == (1 << 22) // 3  # truncation
+    assert L.orc_float_to_fixed(float("nan")) == 0
+    assert L.orc_float_to_fixed(-3.0) == 0
+    assert L.orc_float_to_fixed(2000.0) == 0xFFFFFFFF  # saturates (1024+ does not fit 10 integer bits)
+
+
+def test_isocentre_projects_to_detector_centre():
+    """ProjData of an rx=sx=sy=0 single-module geometry maps the isocentre to (W/2, H/2)."""
+    for W, H in ((64, 48), (37, 29)):
+        gp = O.geom_params(dwidth=W, dheight=H, projections=8, sit=1)
+        pd, go = O.geometry(gp)
+        for d in pd:
+            m = d[:16]
+            u, v, w = m[3], m[7], m[15]
+            assert abs(u / w - W / 2) < 1e-3 and abs(v / w - H / 2) < 1e-3
+
+
+def test_single_voxel_and_wraparound():
+    """One voxel at the isocentre lands as FLOAT_TO_FIXED(value) on one pixel per
+    projection; sums wrap modulo 2^32 (u32 atomics, KernelForward.cl:36)."""
+    W = H = 32
+    gp = O.geom_params(dwidth=W, dheight=H, projections=8, sit=1)
+    pd, go = O.geometry(gp)
+    vol = np.zeros(W * H * W, np.float32)
+    c = W // 2
+    vol[(c * W + c) * W + c] = 3.25
+    origin = list(go.orig)
+    L, k = O.make_launch((0, 0, 0), (W, H, W), origin, [go.vx] * 3, W, H, 0, 8, 1)
+    sums = np.zeros(8 * W * H, np.uint32)
+    O.forward(vol, sums, pd, L)
+    per_img = sums.reshape(8, -1)
+    assert ((per_img > 0).sum(axis=1) == 1).all()
+    assert (per_img.max(axis=1) == int(3.25 * (1 << 22))).all()
+    # wrap: 1000 + 1000 + 1000 ... at one pixel overflows 2^32 (fixed(1000) = 1000 << 22)
+    vol[:] = 0
+    vol[(c * W + np.arange(W)) * W + c] = 1000.0  # the central ray of angle 0 (along z)
+    sums[:] = 0
+    O.forward(vol, sums, pd, L)
+    first = sums.reshape(8, H, W)[0]
+    assert first[H // 2, W // 2] == (W * (1000 << 22)) % (1 << 32)
+    assert first.sum(dtype=np.uint64) == first[H // 2, W // 2]
+
+
+def test_error_known_answers():
+    img = np.array([1.0, 2.0, 0.5, 1e-9, 3.0], np.float32)
+    got = np.array([1.0, 1.0, 2.0, 1.0, 0.0], np.float32)
+    sums = np.array([O.lib().orc_float_to_fixed(float(g)) for g in got], np.uint32)
+    O.error(img, sums, 1.0)
+    r = sums.view(np.float32)
+    eps = np.float32(2.0 ** -22)
+    expect = [0.0, math.log(2.0), math.log(0.25), math.log(float(eps)), math.log(3.0 / float(eps))]
+    np.testing.assert_allclose(r, np.array(expect, np.float32), rtol=3e-7, atol=0)
+
+
+def test_backward_without_contributions_is_nan():
+    W = H = 16
+    gp = O.geom_params(dwidth=W, dheight=H, projections=4, sit=1)
+    pd, go = O.geometry(gp)
+    vol = np.ones(W * H * W, np.float32)
+    far = [go.orig[0], go.orig[1] + 1000.0, go.orig[2]]  # volume moved far along the axis: out of every ray
+    L, k = O.make_launch((0, 0, 0), (W, H, W), far, [go.vx] * 3, W, H, 0, 4, 1)
+    O.backward(vol, np.zeros(4 * W * H, np.float32), pd, L)
+    assert np.isnan(vol).all()
+
+
+def test_fast_and_strict_contracts_agree_closely():
+    """The two arithmetic contracts differ only where a projection falls within a few
+    ulp of a pixel border."""
+    c = make_case("offsets64", sit=1, seed=5)
+    a = oracle_forward(c, O.STRICT)
+    b = oracle_forward(c, O.FAST)
+    assert (a != b).mean() < 1e-3
+    assert abs(float(a.sum(dtype=np.float64)) - float(b.sum(dtype=np.float64))) / float(a.sum(dtype=np.float64)) < 1e-4
+
+
+def test_culling_is_conservative():
+    """method_1c's per-layer angle lists (geometry.hpp:141-171) drop no in-bounds pair:
+    forward over the culled list == forward over every angle of the sub-iteration."""
+    c = make_case("offsets64", sit=0, seed=6)
+    gp, go, W = c["gp"], c["go"], c["W"]
+    P, S = gp.projections, gp.sit
+    all_idx = np.array(list(range(0, P, S)), np.uint16)
+    slots = np.arange(len(all_idx), dtype=np.uint16)
+    for layer in (0, 5, W // 2, go.vheight - 1):
+        lm = np.zeros(64, np.uint16)
+        li = np.zeros(64, np.uint16)
+        n = O.lib().orc_cull_layer(O.C.byref(gp), O.C.byref(go), c["pd_all"], 0, layer, 0, lm, li)
+        vol = c["vol"][: W * W].copy()
+        outs = []
+        for (m, i) in ((lm[:n].copy(), li[:n].copy()), (all_idx, slots)):
+            L, k = O.make_launch((0, layer, 0), (W, layer + 1, W), c["origin"], [go.vx] * 3, c["Wd"], c["Hd"], 0,
+                                 len(slots), 1, list_mvp=m, list_img=i)
+            s = np.zeros(len(slots) * c["Wd"] * c["Hd"], np.uint32)
+            O.forward(vol, s, c["pd_all"], L)
+            outs.append(s)
+        np.testing.assert_array_equal(outs[0], outs[1])
+
+
+def test_exports_match_header(xlib):
+    import os
+    from xpulse_recon_b200 import _lib
+    hdr = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "xpr.h")
+    names = _lib.exported_symbols(hdr)
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(xlib, n)]
+    assert not missing, missing

@@ -1,0 +1,864 @@
+// xpr_kernels.cu -- sm_100a kernels of the iterative cone-beam hot path.
+//
+//   forward   (KernelForward.cl:10-55 / KernelForwardH.cl:8-37)   k_forward_tiled
+//   backward  (KernelBackward.cl:8-40 / KernelBackwardH.cl:8-42) k_backward_tiled
+//   error     (KernelError.cl:8-24, reconstruction_lplh.hpp:140-177) k_error
+//   -log / normalise (data_loader.hpp:48-101)                     k_minmax, k_preprocess
+//
+// Design (B200): the path is a voxel-driven nearest-pixel splat / gather.  It
+// is bound by FP32 issue and atomic throughput, not by HBM bytes, so the
+// kernels are organised to cut atomics and redundant arithmetic:
+//
+//  * A CTA owns a brick of 32 x 8 x 32 voxels (x, y, z) for a run of
+//    projections.  The forward keeps the brick in shared memory as 22-bit
+//    fixed point (loaded once, coalesced), projects its 8 corners per
+//    projection to bound its detector footprint, splats into a shared-memory
+//    tile of that footprint with shared atomics, and flushes the tile with one
+//    coalesced global atomic per touched pixel.  Bricks whose footprint misses
+//    the viewport are skipped; all-zero bricks are skipped.
+//  * Each thread walks one line of voxels along the axis closest to the ray
+//    (x or z, chosen per projection) with its 32 lanes across the ray, so the
+//    lanes of a warp hit distinct pixels, and consecutive voxels on the line
+//    (which mostly land on the same pixel) are summed in a register before an
+//    atomic is issued.  Integer atomics commute, so the result is bit-identical
+//    to the reference's voxel-per-work-item order.
+//  * The backward keeps each voxel's running sum and count in registers and
+//    visits projections in the reference's order, so the floating-point sum is
+//    the reference's sum; detector gathers go through the read-only L1 path,
+//    which the brick's small footprint keeps resident.
+//  * Along a line the per-row projective numerators are affine; the line
+//    invariant part is computed once per line (see xpr_math.cuh for the exact
+//    operation contracts).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cfloat>
+
+#include "xpr_internal.h"
+#include "xpr_math.cuh"
+
+namespace xpr {
+
+constexpr int BX = 32;        // brick extent along x (one warp lane per x in z-lines)
+constexpr int BY = 8;         // brick extent along y (one warp per y)
+constexpr int BZ = 32;        // brick extent along z (forward)
+constexpr int NT = 256;       // threads per CTA
+constexpr int G = 4;          // projections whose tiles are in flight together
+constexpr int TILE_CAP = 1024;  // pixels per shared-memory tile
+constexpr int VSTRIDE = 33;   // padded row stride of the brick value array (bank-conflict free both ways)
+constexpr int BWD_LZ = 16;    // backward line length along z
+
+enum Mode : int { kSkip = 0, kTile = 1, kDirect = 2 };
+
+struct ProjMeta {
+    float cu[4], cv[4], cw[4];  // matrix rows for u, v, w (glm columns c0, c1, c3)
+    float fu0, fu1, fv0, fv1;   // rectangle as floats (FAST bounds)
+    int u0, u1, v0, v1;         // rectangle [u0,u1) x [v0,v1) in buffer coordinates
+    int mode;
+    int orient_x;               // walk lines along x (ray closer to x than to z)
+    uint32_t img_base;          // image slot * det_w * rows
+    int tw;
+};
+
+// --------------------------------------------------------------------------------------
+// per-projection metadata: one group of G entries, computed by warp 0
+// lane = g * 8 + corner
+// --------------------------------------------------------------------------------------
+template <bool LIST>
+__device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdata *__restrict__ pd,
+                                             const LaunchArgs &a, int e0, int e_end, int bx0, int by0, int bz0,
+                                             int depth_z, int lane)
+{
+    const int g = lane >> 3, c = lane & 7;
+    const int entry = e0 + g;
+    bool valid = entry < e_end;
+    uint32_t pidx = 0, img = 0;
+    if (valid) {
+        pidx = LIST ? (uint32_t)__ldg(&a.list_mvp[entry]) : (uint32_t)entry;
+        img = LIST ? (uint32_t)__ldg(&a.list_img[entry]) : (uint32_t)entry / a.modules;
+        valid = pidx < a.n_pd && img < a.n_images;
+    }
+    const float *m = valid ? pd[pidx].mvp : pd[0].mvp;
+    float cu0 = __ldg(m + 0), cu1 = __ldg(m + 1), cu2 = __ldg(m + 2), cu3 = __ldg(m + 3);
+    float cv0 = __ldg(m + 4), cv1 = __ldg(m + 5), cv2 = __ldg(m + 6), cv3 = __ldg(m + 7);
+    float cw0 = __ldg(m + 12), cw1 = __ldg(m + 13), cw2 = __ldg(m + 14), cw3 = __ldg(m + 15);
+    // corner voxel centres of the brick (nominal extent; partial bricks are covered)
+    const int ix = a.vmin[0] + bx0 + ((c & 1) ? BX - 1 : 0);
+    const int iy = a.vmin[1] + by0 + ((c & 2) ? BY - 1 : 0);
+    const int iz = a.vmin[2] + bz0 + ((c & 4) ? depth_z - 1 : 0);
+    const float px = __fmaf_rn((float)ix, a.voxel[0], a.origin[0]);
+    const float py = __fmaf_rn((float)iy, a.voxel[1], a.origin[1]);
+    const float pz = __fmaf_rn((float)iz, a.voxel[2], a.origin[2]);
+    const float nu = __fmaf_rn(cu0, px, __fmaf_rn(cu1, py, __fmaf_rn(cu2, pz, cu3)));
+    const float nv = __fmaf_rn(cv0, px, __fmaf_rn(cv1, py, __fmaf_rn(cv2, pz, cv3)));
+    const float nw = __fmaf_rn(cw0, px, __fmaf_rn(cw1, py, __fmaf_rn(cw2, pz, cw3)));
+    const float u = __fdiv_rn(nu, nw);
+    const float v = __fsub_rn(__fdiv_rn(nv, nw), a.row_off_f);
+    int ok = (nw > 0.0f) && (fabsf(u) < 1.0e9f) && (fabsf(v) < 1.0e9f);
+    float umin = ok ? u : 0.0f, umax = umin, vmn = ok ? v : 0.0f, vmx = vmn;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        umin = fminf(umin, __shfl_xor_sync(0xffffffffu, umin, o));
+        umax = fmaxf(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+        vmn = fminf(vmn, __shfl_xor_sync(0xffffffffu, vmn, o));
+        vmx = fmaxf(vmx, __shfl_xor_sync(0xffffffffu, vmx, o));
+        ok &= __shfl_xor_sync(0xffffffffu, ok, o);
+    }
+    if (c == 0) {
+        ProjMeta &M = s_meta[g];
+        const float *vp = valid ? pd[pidx].vp : pd[0].vp;
+        int l = max((int)ceilf(fmaxf(__ldg(vp + 0), -1.0e9f)), 0);
+        int r = min((int)ceilf(fminf(__ldg(vp + 1), 1.0e9f)), (int)a.det_w);
+        int b = max((int)ceilf(fmaxf(__ldg(vp + 2), -1.0e9f)), 0);
+        int t = min((int)ceilf(fminf(__ldg(vp + 3), 1.0e9f)), (int)a.rows);
+        if (ok) {
+            l = max(l, (int)floorf(umin) - 2);
+            r = min(r, (int)ceilf(umax) + 3);
+            b = max(b, (int)floorf(vmn) - 2);
+            t = min(t, (int)ceilf(vmx) + 3);
+        }
+        M.u0 = l; M.u1 = r; M.v0 = b; M.v1 = t;
+        M.fu0 = (float)l; M.fu1 = (float)r; M.fv0 = (float)b; M.fv1 = (float)t;
+        const int area = (r - l) * (t - b);
+        M.mode = (!valid || r <= l || t <= b) ? kSkip : ((ok && area <= TILE_CAP) ? kTile : kDirect);
+        M.tw = r - l;
+        M.orient_x = fabsf(cw0) > fabsf(cw2);
+        M.img_base = img * a.img_stride;
+        M.cu[0] = cu0; M.cu[1] = cu1; M.cu[2] = cu2; M.cu[3] = cu3;
+        M.cv[0] = cv0; M.cv[1] = cv1; M.cv[2] = cv2; M.cv[3] = cv3;
+        M.cw[0] = cw0; M.cw[1] = cw1; M.cw[2] = cw2; M.cw[3] = cw3;
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// one (voxel, projection) pair in each contract, given the line-invariant terms
+// --------------------------------------------------------------------------------------
+// FAST: n_r = A_r + B_r with A_r = fma(c.x, px, fma(c.y, py, c.w)), B_r = c.z * pz.
+// Returns in-rectangle; (iu_bits, iv_bits) are the float bits of 2^23 + pixel.
+__device__ __forceinline__ bool pair_fast(float nu, float nv, float nw, const ProjMeta &M, float hv,
+                                          uint32_t &iu_bits, uint32_t &iv_bits)
+{
+    const float rw = __frcp_rn(nw);
+    const float yu = __fmaf_rn(nu, rw, 0.5f);
+    const float yv = __fmaf_rn(nv, rw, hv);
+    const bool in = (yu >= M.fu0) && (yu < M.fu1) && (yv >= M.fv0) && (yv < M.fv1);
+    iu_bits = __float_as_uint(__fadd_rz(yu, 8388608.0f));
+    iv_bits = __float_as_uint(__fadd_rz(yv, 8388608.0f));
+    return in;
+}
+
+// STRICT: u = n_u / n_w; v = n_v / n_w - off; round half away; saturating convert.
+__device__ __forceinline__ bool pair_strict(float nu, float nv, float nw, const ProjMeta &M, float off,
+                                            int &cu, int &cv)
+{
+    const float u = __fdiv_rn(nu, nw);
+    const float v = __fsub_rn(__fdiv_rn(nv, nw), off);
+    cu = __float2int_rz(roundf(u));
+    cv = __float2int_rz(roundf(v));
+    return (cu >= M.u0) && (cu < M.u1) && (cv >= M.v0) && (cv < M.v1);
+}
+
+// Line walker: calls f(k, in, tile_index, global_index) for the voxels k = 0..LEN-1 of
+// this thread's line.  ORX: walk along x (lane = z), else along z (lane = x).
+template <int ARITH, bool ORX, int LEN, typename F>
+__device__ __forceinline__ void walk_line(const ProjMeta &M, const LaunchArgs &a, int ax, int ay, int az, F &&f)
+{
+    const float vx = a.voxel[0], vy = a.voxel[1], vz = a.voxel[2];
+    const float ox = a.origin[0], oy = a.origin[1], oz = a.origin[2];
+    const uint32_t W = a.det_w;
+    const uint32_t tw = (uint32_t)M.tw;
+    if (ARITH == kFast) {
+        const float py = __fmaf_rn((float)ay, vy, oy);
+        // tile index = (iv - v0) * tw + (iu - u0) with iu = iu_bits - 0x4B000000
+        const uint32_t ct = 0x4B000000u * (tw + 1u) + (uint32_t)M.v0 * tw + (uint32_t)M.u0;
+        const uint32_t cg = 0x4B000000u * (W + 1u) - M.img_base;
+        if (!ORX) {
+            const float px = __fmaf_rn((float)ax, vx, ox);
+            const float Au = __fmaf_rn(M.cu[0], px, __fmaf_rn(M.cu[1], py, M.cu[3]));
+            const float Av = __fmaf_rn(M.cv[0], px, __fmaf_rn(M.cv[1], py, M.cv[3]));
+            const float Aw = __fmaf_rn(M.cw[0], px, __fmaf_rn(M.cw[1], py, M.cw[3]));
+            const float fz0 = (float)az;
+#pragma unroll
+            for (int k = 0; k < LEN; ++k) {
+                const float pz = __fmaf_rn(__fadd_rn(fz0, (float)k), vz, oz);
+                const float nu = __fadd_rn(Au, __fmul_rn(M.cu[2], pz));
+                const float nv = __fadd_rn(Av, __fmul_rn(M.cv[2], pz));
+                const float nw = __fadd_rn(Aw, __fmul_rn(M.cw[2], pz));
+                uint32_t ub, vb;
+                const bool in = pair_fast(nu, nv, nw, M, a.half_minus_off, ub, vb);
+                f(k, in, vb * tw + ub - ct, vb * W + ub - cg);
+            }
+        } else {
+            const float pz = __fmaf_rn((float)az, vz, oz);
+            const float Ku = __fmaf_rn(M.cu[1], py, M.cu[3]);
+            const float Kv = __fmaf_rn(M.cv[1], py, M.cv[3]);
+            const float Kw = __fmaf_rn(M.cw[1], py, M.cw[3]);
+            const float Bu = __fmul_rn(M.cu[2], pz);
+            const float Bv = __fmul_rn(M.cv[2], pz);
+            const float Bw = __fmul_rn(M.cw[2], pz);
+            const float fx0 = (float)ax;
+#pragma unroll
+            for (int k = 0; k < LEN; ++k) {
+                const float px = __fmaf_rn(__fadd_rn(fx0, (float)k), vx, ox);
+                const float nu = __fadd_rn(__fmaf_rn(M.cu[0], px, Ku), Bu);
+                const float nv = __fadd_rn(__fmaf_rn(M.cv[0], px, Kv), Bv);
+                const float nw = __fadd_rn(__fmaf_rn(M.cw[0], px, Kw), Bw);
+                uint32_t ub, vb;
+                const bool in = pair_fast(nu, nv, nw, M, a.half_minus_off, ub, vb);
+                f(k, in, vb * tw + ub - ct, vb * W + ub - cg);
+            }
+        }
+    } else {
+        // STRICT: p = float(idx) * vx + o;  n = ((c.x*px + c.y*py) + c.z*pz) + c.w
+        const float py = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)ay), vy), oy);
+        const uint32_t ct = (uint32_t)M.v0 * tw + (uint32_t)M.u0;
+        if (!ORX) {
+            const float px = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)ax), vx), ox);
+            const float Pu = __fadd_rn(__fmul_rn(M.cu[0], px), __fmul_rn(M.cu[1], py));
+            const float Pv = __fadd_rn(__fmul_rn(M.cv[0], px), __fmul_rn(M.cv[1], py));
+            const float Pw = __fadd_rn(__fmul_rn(M.cw[0], px), __fmul_rn(M.cw[1], py));
+#pragma unroll
+            for (int k = 0; k < LEN; ++k) {
+                const float pz = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)(az + k)), vz), oz);
+                const float nu = __fadd_rn(__fadd_rn(Pu, __fmul_rn(M.cu[2], pz)), M.cu[3]);
+                const float nv = __fadd_rn(__fadd_rn(Pv, __fmul_rn(M.cv[2], pz)), M.cv[3]);
+                const float nw = __fadd_rn(__fadd_rn(Pw, __fmul_rn(M.cw[2], pz)), M.cw[3]);
+                int cu, cv;
+                const bool in = pair_strict(nu, nv, nw, M, a.row_off_f, cu, cv);
+                f(k, in, (uint32_t)cv * tw + (uint32_t)cu - ct, M.img_base + (uint32_t)cv * W + (uint32_t)cu);
+            }
+        } else {
+            const float pz = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)az), vz), oz);
+            const float Qu = __fmul_rn(M.cu[1], py), Ru = __fmul_rn(M.cu[2], pz);
+            const float Qv = __fmul_rn(M.cv[1], py), Rv = __fmul_rn(M.cv[2], pz);
+            const float Qw = __fmul_rn(M.cw[1], py), Rw = __fmul_rn(M.cw[2], pz);
+#pragma unroll
+            for (int k = 0; k < LEN; ++k) {
+                const float px = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)(ax + k)), vx), ox);
+                const float nu = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(M.cu[0], px), Qu), Ru), M.cu[3]);
+                const float nv = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(M.cv[0], px), Qv), Rv), M.cv[3]);
+                const float nw = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(M.cw[0], px), Qw), Rw), M.cw[3]);
+                int cu, cv;
+                const bool in = pair_strict(nu, nv, nw, M, a.row_off_f, cu, cv);
+                f(k, in, (uint32_t)cv * tw + (uint32_t)cu - ct, M.img_base + (uint32_t)cv * W + (uint32_t)cu);
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// forward
+// --------------------------------------------------------------------------------------
+constexpr size_t kFwdSmem = (size_t)(BY * BZ * VSTRIDE + G * TILE_CAP) * sizeof(uint32_t);
+
+template <int ARITH, bool LIST>
+__global__ void __launch_bounds__(NT, 3)
+    k_forward_tiled(const float *__restrict__ vol, uint32_t *__restrict__ sum, const xpr_projdata *__restrict__ pd,
+                    const LaunchArgs a, int bricks_x, int bricks_z)
+{
+    extern __shared__ uint32_t smem[];
+    uint32_t *s_val = smem;                        // [BY][BZ][VSTRIDE]
+    uint32_t *s_tile = smem + BY * BZ * VSTRIDE;   // [G][TILE_CAP]
+    __shared__ ProjMeta s_meta[G];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int b = blockIdx.x;
+    const int bxi = b % bricks_x;
+    b /= bricks_x;
+    const int bzi = b % bricks_z;
+    const int byi = b / bricks_z;
+    const int x0 = bxi * BX, y0 = byi * BY, z0 = bzi * BZ;
+    const int sx = a.size[0], sy = a.size[1], sz = a.size[2];
+
+    bool any = false;
+    for (int i = threadIdx.x; i < BX * BY * BZ; i += NT) {
+        const int x = i & 31, z = (i >> 5) & 31, y = i >> 10;
+        const int gx = x0 + x, gy = y0 + y, gz = z0 + z;
+        uint32_t v = 0;
+        if (gx < sx && gy < sy && gz < sz) v = float_to_fixed(__ldg(&vol[((size_t)gy * sz + gz) * sx + gx]));
+        s_val[(y * BZ + z) * VSTRIDE + x] = v;
+        any |= (v != 0u);
+    }
+    for (int i = threadIdx.x; i < G * TILE_CAP; i += NT) s_tile[i] = 0u;
+    if (!__syncthreads_or(any)) return;   // an all-zero brick adds nothing
+
+    const int e_begin = blockIdx.y * (int)a.per_split;
+    const int e_end = min((int)a.n_entries, e_begin + (int)a.per_split);
+    const int ay = a.vmin[1] + y0 + warp;
+
+    for (int e0 = e_begin; e0 < e_end; e0 += G) {
+        if (warp == 0) compute_meta<LIST>(s_meta, pd, a, e0, e_end, x0, y0, z0, BZ, lane);
+        __syncthreads();
+#pragma unroll 1
+        for (int g = 0; g < G; ++g) {
+            const ProjMeta &M = s_meta[g];
+            const int mode = M.mode;
+            if (mode == kSkip) continue;
+            uint32_t *tile = s_tile + g * TILE_CAP;
+            uint32_t acc = 0u, prev = 0xffffffffu;
+            auto splat = [&](int k, bool in, uint32_t tidx, uint32_t gidx, uint32_t val) {
+                const uint32_t idx = (mode == kTile) ? tidx : gidx;
+                if (in && idx != prev) {
+                    if (acc) {
+                        if (mode == kTile) atomicAdd(&tile[prev], acc);
+                        else atomicAdd(&sum[prev], acc);
+                    }
+                    acc = 0u;
+                    prev = idx;
+                }
+                acc += in ? val : 0u;
+            };
+            if (M.orient_x) {
+                // lane = z, walk x
+                const uint32_t *row = s_val + (warp * BZ + lane) * VSTRIDE;
+                walk_line<ARITH, true, BX>(M, a, a.vmin[0] + x0, ay, a.vmin[2] + z0 + lane,
+                                           [&](int k, bool in, uint32_t t, uint32_t gi) { splat(k, in, t, gi, row[k]); });
+            } else {
+                // lane = x, walk z
+                const uint32_t *col = s_val + warp * BZ * VSTRIDE + lane;
+                walk_line<ARITH, false, BZ>(M, a, a.vmin[0] + x0 + lane, ay, a.vmin[2] + z0,
+                                            [&](int k, bool in, uint32_t t, uint32_t gi) {
+                                                splat(k, in, t, gi, col[k * VSTRIDE]);
+                                            });
+            }
+            if (acc) {
+                if (mode == kTile) atomicAdd(&tile[prev], acc);
+                else atomicAdd(&sum[prev], acc);
+            }
+        }
+        __syncthreads();
+        // flush the tiles: one global atomic per touched pixel, coalesced along rows
+#pragma unroll 1
+        for (int g = 0; g < G; ++g) {
+            const ProjMeta &M = s_meta[g];
+            if (M.mode != kTile) continue;
+            uint32_t *tile = s_tile + g * TILE_CAP;
+            const int tw = M.tw, th = M.v1 - M.v0;
+            for (int r = warp; r < th; r += NT / 32) {
+                uint32_t *dst = sum + M.img_base + (uint32_t)(M.v0 + r) * a.det_w + (uint32_t)M.u0;
+                for (int c = lane; c < tw; c += 32) {
+                    const uint32_t v = tile[r * tw + c];
+                    if (v) {
+                        tile[r * tw + c] = 0u;
+                        atomicAdd(dst + c, v);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Work-items of the reference NDRange padding (kernel.hpp:73-81, H5): one thread each,
+// voxel coordinates from to3D() (utils.cl:39-45), all projections, global atomics.
+template <int ARITH, bool LIST, bool FWD, bool NANSKIP, int DT>
+__global__ void k_pad_items(float *vol, uint32_t *sum, const void *ratio, const xpr_projdata *__restrict__ pd,
+                            const LaunchArgs a, uint64_t id_begin, uint64_t id_end)
+{
+    const uint64_t id = id_begin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (id >= id_end) return;
+    const uint64_t sx = (uint64_t)a.size[0], sz = (uint64_t)a.size[2];
+    const uint64_t yy = id / (sx * sz), rem = id - yy * sx * sz;
+    const int ax = a.vmin[0] + (int)(rem % sx), az = a.vmin[2] + (int)(rem / sx), ay = a.vmin[1] + (int)yy;
+    float px, py, pz;
+    if (ARITH == kFast) {
+        px = __fmaf_rn((float)ax, a.voxel[0], a.origin[0]);
+        py = __fmaf_rn((float)ay, a.voxel[1], a.origin[1]);
+        pz = __fmaf_rn((float)az, a.voxel[2], a.origin[2]);
+    } else {
+        px = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)ax), a.voxel[0]), a.origin[0]);
+        py = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)ay), a.voxel[1]), a.origin[1]);
+        pz = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)az), a.voxel[2]), a.origin[2]);
+    }
+    const uint32_t value = FWD ? float_to_fixed(vol[id]) : 0u;
+    float s = 0.0f;
+    uint32_t cnt = 0u;
+    for (uint32_t e = 0; e < a.n_entries; ++e) {
+        const uint32_t pidx = LIST ? (uint32_t)a.list_mvp[e] : e;
+        const uint32_t img = LIST ? (uint32_t)a.list_img[e] : e / a.modules;
+        if (pidx >= a.n_pd || img >= a.n_images) continue;
+        const float *m = pd[pidx].mvp;
+        const float *vp = pd[pidx].vp;
+        const int l = max((int)ceilf(vp[0]), 0), r = min((int)ceilf(vp[1]), (int)a.det_w);
+        const int bb = max((int)ceilf(vp[2]), 0), t = min((int)ceilf(vp[3]), (int)a.rows);
+        int iu, iv;
+        bool in;
+        if (ARITH == kFast) {
+            const float nu = __fadd_rn(__fmaf_rn(m[0], px, __fmaf_rn(m[1], py, m[3])), __fmul_rn(m[2], pz));
+            const float nv = __fadd_rn(__fmaf_rn(m[4], px, __fmaf_rn(m[5], py, m[7])), __fmul_rn(m[6], pz));
+            const float nw = __fadd_rn(__fmaf_rn(m[12], px, __fmaf_rn(m[13], py, m[15])), __fmul_rn(m[14], pz));
+            const float rw = __frcp_rn(nw);
+            const float yu = __fmaf_rn(nu, rw, 0.5f), yv = __fmaf_rn(nv, rw, a.half_minus_off);
+            in = yu >= (float)l && yu < (float)r && yv >= (float)bb && yv < (float)t;
+            iu = in ? (int)floorf(yu) : 0;
+            iv = in ? (int)floorf(yv) : 0;
+        } else {
+            const float nu = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], px), __fmul_rn(m[1], py)), __fmul_rn(m[2], pz)), m[3]);
+            const float nv = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[4], px), __fmul_rn(m[5], py)), __fmul_rn(m[6], pz)), m[7]);
+            const float nw = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[12], px), __fmul_rn(m[13], py)), __fmul_rn(m[14], pz)), m[15]);
+            iu = __float2int_rz(roundf(__fdiv_rn(nu, nw)));
+            iv = __float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), a.row_off_f)));
+            in = iu >= l && iu < r && iv >= bb && iv < t;
+        }
+        if (!in) continue;
+        const uint32_t gi = img * a.img_stride + (uint32_t)iv * a.det_w + (uint32_t)iu;
+        if (FWD) {
+            atomicAdd(&sum[gi], value);
+        } else {
+            float rr;
+            if (DT == kF32) rr = ((const float *)ratio)[gi];
+            else if (DT == kBF16) rr = __bfloat162float(((const __nv_bfloat16 *)ratio)[gi]);
+            else rr = __half2float(((const __half *)ratio)[gi]);
+            if (NANSKIP && rr != rr) continue;
+            s = __fadd_rn(s, rr);
+            cnt += 1u;
+        }
+    }
+    if (!FWD) vol[id] = __fmul_rn(vol[id], p_expf(__fdiv_rn(s, __uint2float_rn(cnt))));
+}
+
+// --------------------------------------------------------------------------------------
+// backward
+// --------------------------------------------------------------------------------------
+template <int DT>
+__device__ __forceinline__ float load_ratio(const void *ratio, uint32_t i)
+{
+    if (DT == kF32) return __ldg((const float *)ratio + i);
+    if (DT == kBF16) return __bfloat162float(__ldg((const __nv_bfloat16 *)ratio + i));
+    return __half2float(__ldg((const __half *)ratio + i));
+}
+
+template <int ARITH, bool LIST, bool NANSKIP, int DT>
+__global__ void __launch_bounds__(NT, 2)
+    k_backward_tiled(float *__restrict__ vol, const void *__restrict__ ratio, const xpr_projdata *__restrict__ pd,
+                     const LaunchArgs a, int bricks_x, int bricks_z)
+{
+    __shared__ ProjMeta s_meta[G];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int b = blockIdx.x;
+    const int bxi = b % bricks_x;
+    b /= bricks_x;
+    const int bzi = b % bricks_z;
+    const int byi = b / bricks_z;
+    const int x0 = bxi * BX, y0 = byi * BY, z0 = bzi * BWD_LZ;
+    const int ax = a.vmin[0] + x0 + lane, ay = a.vmin[1] + y0 + warp, az = a.vmin[2] + z0;
+
+    float s[BWD_LZ];
+    uint32_t n[BWD_LZ];
+#pragma unroll
+    for (int k = 0; k < BWD_LZ; ++k) { s[k] = 0.0f; n[k] = 0u; }
+
+    for (int e0 = 0; e0 < (int)a.n_entries; e0 += G) {
+        if (warp == 0) compute_meta<LIST>(s_meta, pd, a, e0, (int)a.n_entries, x0, y0, z0, BWD_LZ, lane);
+        __syncthreads();
+#pragma unroll 1
+        for (int g = 0; g < G; ++g) {
+            const ProjMeta &M = s_meta[g];
+            if (M.mode == kSkip) continue;
+            walk_line<ARITH, false, BWD_LZ>(M, a, ax, ay, az, [&](int k, bool in, uint32_t, uint32_t gi) {
+                if (in) {
+                    const float r = load_ratio<DT>(ratio, gi);
+                    if (!NANSKIP || r == r) {
+                        s[k] = __fadd_rn(s[k], r);
+                        n[k] += 1u;
+                    }
+                }
+            });
+        }
+        __syncthreads();
+    }
+    const int sx = a.size[0], sy = a.size[1], sz = a.size[2];
+    const int x = x0 + lane, y = y0 + warp;
+    if (x >= sx || y >= sy) return;
+#pragma unroll
+    for (int k = 0; k < BWD_LZ; ++k) {
+        const int z = z0 + k;
+        if (z < sz) {
+            float *p = vol + ((size_t)y * sz + z) * sx + x;
+            *p = __fmul_rn(*p, p_expf(__fdiv_rn(s[k], __uint2float_rn(n[k]))));
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// error, preprocessing, fill
+// --------------------------------------------------------------------------------------
+template <int DT>
+__device__ __forceinline__ float load_any(const void *p, uint64_t i)
+{
+    if (DT == kF32) return ((const float *)p)[i];
+    if (DT == kBF16) return __bfloat162float(((const __nv_bfloat16 *)p)[i]);
+    return __half2float(((const __half *)p)[i]);
+}
+template <int DT>
+__device__ __forceinline__ void store_any(void *p, uint64_t i, float v)
+{
+    if (DT == kF32) ((float *)p)[i] = v;
+    else if (DT == kBF16) ((__nv_bfloat16 *)p)[i] = __float2bfloat16_rn(v);
+    else ((__half *)p)[i] = __float2half_rn(v);
+}
+__device__ __forceinline__ float std_max(float a, float b) { return (a < b) ? b : a; }
+
+template <int MODE, int IDT, int RDT, bool ZERO, bool RESID>
+__global__ void k_error(const void *__restrict__ images, uint32_t *sum, void *ratio, uint64_t n, float w,
+                        double *residual)
+{
+    double acc = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float ref = load_any<IDT>(images, i);
+        const float got = fixed_to_float(sum[i]);
+        float r;
+        if (MODE == XPR_ERROR_STD) r = __fmul_rn(p_logf(fmaxf(__fdiv_rn(ref, fmaxf(got, kEps)), kEps)), w);
+        else if (MODE == XPR_ERROR_FIRST_1C) r = p_logf(std_max(ref, kEps));
+        else r = __fmul_rn(p_logf(std_max(__fdiv_rn(ref, std_max(got, kEps)), kEps)), w);
+        store_any<RDT>(ratio, i, r);
+        if (ZERO) sum[i] = 0u;
+        if (RESID) acc += (double)r * (double)r;
+    }
+    if (RESID) {
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(residual, acc);
+    }
+}
+
+// order-preserving float <-> int map for atomic min / max
+__device__ __forceinline__ int ford(float f)
+{
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float fordinv(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+__device__ __forceinline__ bool is_normal(float v)
+{
+    const uint32_t e = (__float_as_uint(v) >> 23) & 0xffu;
+    return e != 0u && e != 0xffu;
+}
+
+__global__ void k_minmax(const float *__restrict__ x, uint64_t n, float *minmax)
+{
+    float mn = FLT_MAX, mx = -FLT_MAX;
+    bool anyv = false;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float v = x[i];
+        if (is_normal(v)) {
+            mn = fminf(mn, v);
+            mx = fmaxf(mx, v);
+            anyv = true;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    anyv = __any_sync(0xffffffffu, anyv);
+    if ((threadIdx.x & 31) == 0 && anyv) {
+        atomicMin((int *)&minmax[0], ford(mn));
+        atomicMax((int *)&minmax[1], ford(mx));
+    }
+}
+
+// minmax[] holds ford()-encoded values while the reduction runs
+__global__ void k_minmax_encode(float *minmax, bool decode)
+{
+    if (threadIdx.x == 0) {
+        if (!decode) {
+            const int a = ford(minmax[0]), b = ford(minmax[1]);
+            ((int *)minmax)[0] = a;
+            ((int *)minmax)[1] = b;
+        } else {
+            const float a = fordinv(((int *)minmax)[0]), b = fordinv(((int *)minmax)[1]);
+            minmax[0] = a;
+            minmax[1] = b;
+        }
+    }
+}
+
+template <int ODT>
+__global__ void k_preprocess(const float *__restrict__ x, void *out, uint64_t n, int normalize,
+                             const float *__restrict__ minmax, int mlog)
+{
+    const float mn = normalize ? minmax[0] : 0.0f, mx = normalize ? minmax[1] : 0.0f;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        float v = x[i];
+        if (normalize) v = is_normal(v) ? __fdiv_rn(__fsub_rn(v, mn), __fsub_rn(mx, mn)) : __fdiv_rn(__fadd_rn(mx, mn), 2.0f);
+        if (mlog) {
+            const float lo = 1.0f - kEps;
+            float c = (lo < v) ? lo : v;          // std::min(v, 1 - eps)
+            c = (c < kEps) ? kEps : c;            // std::max(., eps)
+            v = -p_logf(c);
+        }
+        store_any<ODT>(out, i, v);
+    }
+}
+
+__global__ void k_fill_u32(uint32_t *dst, uint32_t value, uint64_t count)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = value;
+}
+
+template <int ODT>
+__global__ void k_convert(const float *__restrict__ x, void *out, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        store_any<ODT>(out, i, x[i]);
+}
+
+// ======================================================================================
+// launchers
+// ======================================================================================
+static inline unsigned stream_grid(uint64_t n, const DeviceInfo &dev)
+{
+    const uint64_t want = (n + 255) / 256;
+    const uint64_t cap = (uint64_t)dev.sm_count * 8;
+    return (unsigned)std::max<uint64_t>(1, std::min(want, cap));
+}
+
+const char *make_launch_args(const xpr_launch *L, uint32_t n_pd, LaunchArgs *a)
+{
+    if (!L) return "launch descriptor is NULL";
+    for (int i = 0; i < 3; ++i) {
+        if (L->vmin[i] < 0 || L->vmax[i] <= L->vmin[i]) return "volume box must satisfy 0 <= vmin < vmax";
+        a->vmin[i] = L->vmin[i];
+        a->size[i] = L->vmax[i] - L->vmin[i];
+        a->origin[i] = L->origin[i];
+        a->voxel[i] = L->voxel[i];
+    }
+    if (L->det_w == 0 || L->rows == 0) return "detector width and rows must be positive";
+    if (L->det_w > (1u << 22) || L->rows > (1u << 22)) return "detector width / rows exceed 2^22";
+    if (L->row_offset < 0 || L->row_offset > (1 << 22)) return "row_offset must be in [0, 2^22]";
+    if (L->arith != XPR_ARITH_STRICT && L->arith != XPR_ARITH_FAST) return "unknown arith mode";
+    if (n_pd == 0) return "no ProjData";
+    const uint32_t M = L->modules ? L->modules : 1u;
+    a->det_w = L->det_w;
+    a->rows = L->rows;
+    a->row_off_f = (float)(uint32_t)L->row_offset;
+    a->half_minus_off = 0.5f - (float)L->row_offset;
+    a->modules = M;
+    a->n_pd = n_pd;
+    a->img_stride = L->det_w * L->rows;
+    if (L->list_mvp || L->list_img) {
+        if (!L->list_mvp || !L->list_img) return "both index lists are required";
+        a->list_mvp = L->list_mvp;
+        a->list_img = L->list_img;
+        a->n_entries = L->n_list;
+        a->n_images = L->n_angles;
+    } else {
+        a->list_mvp = nullptr;
+        a->list_img = nullptr;
+        if ((uint64_t)L->n_angles * M > n_pd) return "n_angles * modules exceeds the ProjData count";
+        a->n_entries = L->n_angles * M;
+        a->n_images = L->n_angles;
+    }
+    if ((uint64_t)a->img_stride * a->n_images >= (1ull << 32)) return "detector buffer exceeds 2^32 elements";
+    const uint64_t nvox = (uint64_t)a->size[0] * a->size[1] * a->size[2];
+    if (nvox + 64 >= (1ull << 40)) return "volume box too large";
+    a->per_split = a->n_entries;
+    return nullptr;
+}
+
+static bool g_attr_done[64];
+
+cudaError_t prepare_device_kernels()
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && g_attr_done[dev]) return cudaSuccess;
+    const int smem = (int)kFwdSmem;
+    void (*fns[])(const float *, uint32_t *, const xpr_projdata *, const LaunchArgs, int, int) = {
+        k_forward_tiled<kStrict, false>, k_forward_tiled<kStrict, true>, k_forward_tiled<kFast, false>,
+        k_forward_tiled<kFast, true>};
+    for (auto f : fns) {
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+    }
+    if (dev < 64) g_attr_done[dev] = true;
+    return cudaSuccess;
+}
+
+cudaError_t launch_forward(const float *vol, uint32_t *sum, const xpr_projdata *pd, const LaunchArgs &a0, int arith,
+                           int compat_pad, const DeviceInfo &dev, cudaStream_t s)
+{
+    cudaError_t e = prepare_device_kernels();
+    if (e != cudaSuccess) return e;
+    LaunchArgs a = a0;
+    const int bx = (a.size[0] + BX - 1) / BX, by = (a.size[1] + BY - 1) / BY, bz = (a.size[2] + BZ - 1) / BZ;
+    const uint64_t bricks = (uint64_t)bx * by * bz;
+    // split the projection run across CTAs when the volume has too few bricks to fill the GPU
+    const uint64_t target = (uint64_t)dev.sm_count * 3 * 4;
+    uint32_t splits = 1;
+    if (bricks < target && a.n_entries > (uint32_t)G) {
+        splits = (uint32_t)std::min<uint64_t>((target + bricks - 1) / bricks, (a.n_entries + G - 1) / G);
+        splits = std::max<uint32_t>(splits, 1);
+    }
+    a.per_split = (((a.n_entries + splits - 1) / splits) + G - 1) / G * G;
+    splits = (a.n_entries + a.per_split - 1) / std::max<uint32_t>(a.per_split, 1);
+    if (splits == 0) splits = 1;
+    if (a.n_entries > 0 && bricks > 0) {
+        dim3 grid((unsigned)bricks, splits);
+        const bool list = a.list_mvp != nullptr;
+        if (arith == kFast) {
+            if (list) k_forward_tiled<kFast, true><<<grid, NT, kFwdSmem, s>>>(vol, sum, pd, a, bx, bz);
+            else k_forward_tiled<kFast, false><<<grid, NT, kFwdSmem, s>>>(vol, sum, pd, a, bx, bz);
+        } else {
+            if (list) k_forward_tiled<kStrict, true><<<grid, NT, kFwdSmem, s>>>(vol, sum, pd, a, bx, bz);
+            else k_forward_tiled<kStrict, false><<<grid, NT, kFwdSmem, s>>>(vol, sum, pd, a, bx, bz);
+        }
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (compat_pad && a.n_entries > 0) {
+        const uint64_t n = (uint64_t)a.size[0] * a.size[1] * a.size[2];
+        const uint64_t end = n + (32u - n % 32u);
+        const unsigned blocks = (unsigned)((end - n + 63) / 64);
+        const bool list = a.list_mvp != nullptr;
+#define XPR_PAD_FWD(AR, LI) k_pad_items<AR, LI, true, false, kF32><<<blocks, 64, 0, s>>>(const_cast<float *>(vol), sum, nullptr, pd, a, n, end)
+        if (arith == kFast) { if (list) XPR_PAD_FWD(kFast, true); else XPR_PAD_FWD(kFast, false); }
+        else { if (list) XPR_PAD_FWD(kStrict, true); else XPR_PAD_FWD(kStrict, false); }
+#undef XPR_PAD_FWD
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+template <int AR, bool LI, bool NS>
+static void dispatch_bwd_dt(int dt, dim3 grid, cudaStream_t s, float *vol, const void *ratio, const xpr_projdata *pd,
+                            const LaunchArgs &a, int bx, int bz)
+{
+    if (dt == kBF16) k_backward_tiled<AR, LI, NS, kBF16><<<grid, NT, 0, s>>>(vol, ratio, pd, a, bx, bz);
+    else if (dt == kF16) k_backward_tiled<AR, LI, NS, kF16><<<grid, NT, 0, s>>>(vol, ratio, pd, a, bx, bz);
+    else k_backward_tiled<AR, LI, NS, kF32><<<grid, NT, 0, s>>>(vol, ratio, pd, a, bx, bz);
+}
+
+template <int AR, bool LI, bool NS>
+static void dispatch_pad_bwd_dt(int dt, unsigned blocks, cudaStream_t s, float *vol, const void *ratio,
+                                const xpr_projdata *pd, const LaunchArgs &a, uint64_t b, uint64_t e)
+{
+    if (dt == kBF16) k_pad_items<AR, LI, false, NS, kBF16><<<blocks, 64, 0, s>>>(vol, nullptr, ratio, pd, a, b, e);
+    else if (dt == kF16) k_pad_items<AR, LI, false, NS, kF16><<<blocks, 64, 0, s>>>(vol, nullptr, ratio, pd, a, b, e);
+    else k_pad_items<AR, LI, false, NS, kF32><<<blocks, 64, 0, s>>>(vol, nullptr, ratio, pd, a, b, e);
+}
+
+cudaError_t launch_backward(float *vol, const void *ratio, int dt, const xpr_projdata *pd, const LaunchArgs &a,
+                            int arith, int compat_pad, int nan_skip, const DeviceInfo &dev, cudaStream_t s)
+{
+    (void)dev;
+    const int bx = (a.size[0] + BX - 1) / BX, by = (a.size[1] + BY - 1) / BY, bz = (a.size[2] + BWD_LZ - 1) / BWD_LZ;
+    const uint64_t bricks = (uint64_t)bx * by * bz;
+    const bool list = a.list_mvp != nullptr;
+    dim3 grid((unsigned)bricks);
+    if (bricks > 0) {
+#define XPR_BWD(AR, LI, NS) dispatch_bwd_dt<AR, LI, NS>(dt, grid, s, vol, ratio, pd, a, bx, bz)
+        if (arith == kFast) {
+            if (list) { if (nan_skip) XPR_BWD(kFast, true, true); else XPR_BWD(kFast, true, false); }
+            else { if (nan_skip) XPR_BWD(kFast, false, true); else XPR_BWD(kFast, false, false); }
+        } else {
+            if (list) { if (nan_skip) XPR_BWD(kStrict, true, true); else XPR_BWD(kStrict, true, false); }
+            else { if (nan_skip) XPR_BWD(kStrict, false, true); else XPR_BWD(kStrict, false, false); }
+        }
+#undef XPR_BWD
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (compat_pad) {
+        const uint64_t n = (uint64_t)a.size[0] * a.size[1] * a.size[2];
+        const uint64_t end = n + (32u - n % 32u);
+        const unsigned blocks = (unsigned)((end - n + 63) / 64);
+#define XPR_PADB(AR, LI, NS) dispatch_pad_bwd_dt<AR, LI, NS>(dt, blocks, s, vol, ratio, pd, a, n, end)
+        if (arith == kFast) {
+            if (list) { if (nan_skip) XPR_PADB(kFast, true, true); else XPR_PADB(kFast, true, false); }
+            else { if (nan_skip) XPR_PADB(kFast, false, true); else XPR_PADB(kFast, false, false); }
+        } else {
+            if (list) { if (nan_skip) XPR_PADB(kStrict, true, true); else XPR_PADB(kStrict, true, false); }
+            else { if (nan_skip) XPR_PADB(kStrict, false, true); else XPR_PADB(kStrict, false, false); }
+        }
+#undef XPR_PADB
+        return cudaGetLastError();
+    }
+    return cudaSuccess;
+}
+
+template <int MODE, int IDT, int RDT>
+static void dispatch_error3(unsigned grid, cudaStream_t s, const void *img, uint32_t *sum, void *ratio, uint64_t n,
+                            float w, bool zero, double *res)
+{
+    if (zero) {
+        if (res) k_error<MODE, IDT, RDT, true, true><<<grid, 256, 0, s>>>(img, sum, ratio, n, w, res);
+        else k_error<MODE, IDT, RDT, true, false><<<grid, 256, 0, s>>>(img, sum, ratio, n, w, res);
+    } else {
+        if (res) k_error<MODE, IDT, RDT, false, true><<<grid, 256, 0, s>>>(img, sum, ratio, n, w, res);
+        else k_error<MODE, IDT, RDT, false, false><<<grid, 256, 0, s>>>(img, sum, ratio, n, w, res);
+    }
+}
+
+template <int MODE, int IDT>
+static void dispatch_error2(int rdt, unsigned grid, cudaStream_t s, const void *img, uint32_t *sum, void *ratio,
+                            uint64_t n, float w, bool zero, double *res)
+{
+    if (rdt == kBF16) dispatch_error3<MODE, IDT, kBF16>(grid, s, img, sum, ratio, n, w, zero, res);
+    else if (rdt == kF16) dispatch_error3<MODE, IDT, kF16>(grid, s, img, sum, ratio, n, w, zero, res);
+    else dispatch_error3<MODE, IDT, kF32>(grid, s, img, sum, ratio, n, w, zero, res);
+}
+
+template <int MODE>
+static void dispatch_error1(int idt, int rdt, unsigned grid, cudaStream_t s, const void *img, uint32_t *sum,
+                            void *ratio, uint64_t n, float w, bool zero, double *res)
+{
+    if (idt == kBF16) dispatch_error2<MODE, kBF16>(rdt, grid, s, img, sum, ratio, n, w, zero, res);
+    else if (idt == kF16) dispatch_error2<MODE, kF16>(rdt, grid, s, img, sum, ratio, n, w, zero, res);
+    else dispatch_error2<MODE, kF32>(rdt, grid, s, img, sum, ratio, n, w, zero, res);
+}
+
+cudaError_t launch_error(const void *images, int idt, uint32_t *sum, void *ratio, int rdt, uint64_t n, float weight,
+                         int mode, int zero_sum, double *residual, const DeviceInfo &dev, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const unsigned grid = stream_grid(n, dev);
+    const bool zero = zero_sum && ((void *)sum != ratio);
+    if (mode == XPR_ERROR_FIRST_1C) dispatch_error1<XPR_ERROR_FIRST_1C>(idt, rdt, grid, s, images, sum, ratio, n, weight, zero, residual);
+    else if (mode == XPR_ERROR_1C) dispatch_error1<XPR_ERROR_1C>(idt, rdt, grid, s, images, sum, ratio, n, weight, zero, residual);
+    else dispatch_error1<XPR_ERROR_STD>(idt, rdt, grid, s, images, sum, ratio, n, weight, zero, residual);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_minmax(const float *images, uint64_t n, float *minmax, const DeviceInfo &dev, cudaStream_t s)
+{
+    k_minmax_encode<<<1, 32, 0, s>>>(minmax, false);
+    if (n) k_minmax<<<stream_grid(n, dev), 256, 0, s>>>(images, n, minmax);
+    k_minmax_encode<<<1, 32, 0, s>>>(minmax, true);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_preprocess(const float *images, void *out, int odt, uint64_t n, int normalize, const float *minmax,
+                              int mlog, const DeviceInfo &dev, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const unsigned grid = stream_grid(n, dev);
+    if (odt == kBF16) k_preprocess<kBF16><<<grid, 256, 0, s>>>(images, out, n, normalize, minmax, mlog);
+    else if (odt == kF16) k_preprocess<kF16><<<grid, 256, 0, s>>>(images, out, n, normalize, minmax, mlog);
+    else k_preprocess<kF32><<<grid, 256, 0, s>>>(images, out, n, normalize, minmax, mlog);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_u32(void *dst, uint32_t value, uint64_t count, const DeviceInfo &dev, cudaStream_t s)
+{
+    if (count == 0) return cudaSuccess;
+    if (value == 0u) return cudaMemsetAsync(dst, 0, count * 4, s);
+    k_fill_u32<<<stream_grid(count, dev), 256, 0, s>>>((uint32_t *)dst, value, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(const float *src, void *dst, int dtype, uint64_t n, const DeviceInfo &dev, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const unsigned grid = stream_grid(n, dev);
+    if (dtype == kBF16) k_convert<kBF16><<<grid, 256, 0, s>>>(src, dst, n);
+    else if (dtype == kF16) k_convert<kF16><<<grid, 256, 0, s>>>(src, dst, n);
+    else return cudaMemcpyAsync(dst, src, n * 4, cudaMemcpyDeviceToDevice, s);
+    return cudaGetLastError();
+}
+
+}  // namespace xpr
