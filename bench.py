@@ -38,6 +38,10 @@ CONFIGS = {
                     "720 projections of 768x768, sit=10 -> 72 per sub-iteration",
                dwidth=768, dheight=768, projections=720, sit=10, px=0.1, so=100.0, sd=1000.0, rx=1.5, sx=-2.0,
                sy=3.0, phantom=512, ellipsoids=40, background=0.05, i0=1e5, seed=2),
+    # the c2 geometry restricted to the central 256 layers (profiling-sized: ~3 GB on the device)
+    "c2slab": dict(desc="c2 geometry, central 256-layer y-slab of the 768^3 grid, 72 projections per sub-iteration",
+                   dwidth=768, dheight=768, projections=720, sit=10, px=0.1, so=100.0, sd=1000.0, rx=1.5, sx=-2.0,
+                   sy=3.0, phantom=512, ellipsoids=40, background=0.05, i0=1e5, seed=2, slab=(256, 512)),
     "c1": dict(desc="192^3 recon grid (128^3 phantom: 10 ellipsoids), 180 projections of 192x192, sit=10 -> 18",
                dwidth=192, dheight=192, projections=180, sit=10, px=0.1, so=100.0, sd=1000.0, rx=0.0, sx=0.0,
                sy=0.0, phantom=128, ellipsoids=10, background=0.0, i0=1e5, seed=1),
@@ -127,12 +131,15 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- synthetic data
-def make_phantom(cfg, vx, W, Hv, device, seed):
+def make_phantom(cfg, vx, W, Hv, device, seed, y0=0, y1=None):
     """Seeded ellipsoid phantom (+ smooth Gaussian-textured background) in the central
-    phantom^3 region of the (y, z, x) grid; values are attenuation per voxel (mu * vx)."""
+    phantom^3 region of the (y, z, x) grid; values are attenuation per voxel (mu * vx).
+    Only layers [y0, y1) are materialised."""
     import torch
     rng = np.random.default_rng(seed)
-    vol = torch.zeros((Hv, W, W), dtype=torch.float32, device=device)
+    y1 = Hv if y1 is None else y1
+    full = torch.zeros((Hv, W, W), dtype=torch.float32, device=device) if (y0, y1) == (0, Hv) else None
+    vol = full if full is not None else torch.zeros((y1 - y0, W, W), dtype=torch.float32, device=device)
     ph = cfg["phantom"]
     c0 = np.array([W / 2.0, Hv / 2.0, W / 2.0])  # x, y, z centre in voxels
     mus = []
@@ -158,7 +165,9 @@ def make_phantom(cfg, vx, W, Hv, device, seed):
         Y, Z, X = torch.meshgrid(ys, zs, xs, indexing="ij")
         P = torch.stack([X, Y, Z], dim=-1) @ torch.from_numpy(q.astype(np.float32)).to(device)
         inside = ((P / torch.from_numpy(axes.astype(np.float32)).to(device)) ** 2).sum(-1) <= 1.0
-        vol[lo[1]:hi[1], lo[2]:hi[2], lo[0]:hi[0]] += inside.float() * float(mu * vx)
+        a, b = max(lo[1], y0), min(hi[1], y1)
+        if a < b:
+            vol[a - y0:b - y0, lo[2]:hi[2], lo[0]:hi[0]] += inside[a - lo[1]:b - lo[1]].float() * float(mu * vx)
         del Y, Z, X, P, inside
     if cfg["background"] > 0:
         g = torch.Generator(device=device).manual_seed(seed)
@@ -172,8 +181,10 @@ def make_phantom(cfg, vx, W, Hv, device, seed):
         noise = noise / noise.std()
         level = cfg["background"] * float(np.mean(mus)) * vx
         bg = torch.clamp(level * (1.0 + noise), min=0.0)
-        y0, x0 = (Hv - ph) // 2, (W - ph) // 2
-        vol[y0:y0 + ph, x0:x0 + ph, x0:x0 + ph] += bg
+        py0, x0 = (Hv - ph) // 2, (W - ph) // 2
+        a, b = max(py0, y0), min(py0 + ph, y1)
+        if a < b:
+            vol[a - y0:b - y0, x0:x0 + ph, x0:x0 + ph] += bg[a - py0:b - py0]
         del noise, bg
     return vol.reshape(-1).contiguous()
 
@@ -197,7 +208,8 @@ class Problem:
         self.P, self.S = cfg["projections"], cfg["sit"]
         self.Pc, self.W, self.Hv = self.g["concurrent"], self.g["vwidth"], self.g["vheight"]
         self.Wd, self.Hd = cfg["dwidth"], cfg["dheight"]
-        self.nvox = self.W * self.Hv * self.W
+        self.y0, self.y1 = cfg.get("slab", (0, self.Hv))
+        self.nvox = self.W * (self.y1 - self.y0) * self.W
         self.npix = self.Pc * self.Wd * self.Hd
         self.jitter = JitterSource(seed)
         self.stream = torch.cuda.Stream(device=self.device)
@@ -209,7 +221,7 @@ class Problem:
             self.pd_sub.append(torch.from_numpy(np.ascontiguousarray(self.pd_all[idx])).to(d))
         # measured projections: simulate with the forward projector, Poisson noise, -log on the GPU
         with torch.cuda.stream(self.stream):
-            phantom = make_phantom(cfg, self.g["vx"], self.W, self.Hv, d, seed)
+            phantom = make_phantom(cfg, self.g["vx"], self.W, self.Hv, d, seed, self.y0, self.y1)
             self.images = []
             sums = torch.zeros(self.npix, dtype=torch.int32, device=d)
             gen = torch.Generator(device=d).manual_seed(seed + 1)
@@ -239,8 +251,8 @@ class Problem:
     def launch_desc(self, origin):
         from xpulse_recon_b200 import _lib
         L = _lib.Launch()
-        L.vmin[:] = [0, 0, 0]
-        L.vmax[:] = [self.W, self.Hv, self.W]
+        L.vmin[:] = [0, self.y0, 0]
+        L.vmax[:] = [self.W, self.y1, self.W]
         L.origin[:] = origin
         L.voxel[:] = [self.g["vx"]] * 3
         L.det_w, L.rows, L.row_offset = self.Wd, self.Hd, 0
@@ -414,7 +426,8 @@ def run_ours(args, cfg, rank, world, local):
     for s in range(prob.S):
         hp = C.c_void_p()
         _lib.check(L.xpr_alloc_pinned(prob.ctx.handle, nbytes, C.byref(hp)), "alloc_pinned")
-        C.memmove(hp, prob.images[s].cpu().numpy().ctypes.data, nbytes)
+        host = prob.images[s].view(torch.uint8).cpu().numpy()  # keep alive across the copy
+        C.memmove(hp, host.ctypes.data, nbytes)
         pinned.append(hp)
     res_host = C.c_void_p()
     _lib.check(L.xpr_alloc_pinned(prob.ctx.handle, 8, C.byref(res_host)), "alloc_pinned")
@@ -486,7 +499,7 @@ def run_ours(args, cfg, rank, world, local):
         "value": value, "unit": "GUPS", "n_gpus": world, "steps": K, "warmup": Wm,
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.config + ": " + cfg["desc"], "grid": [prob.W, prob.Hv, prob.W],
+        "config": {"workload": args.config + ": " + cfg["desc"], "grid": [prob.W, prob.y1 - prob.y0, prob.W],
                    "projections": prob.P, "sit": prob.S, "per_subiteration": prob.Pc, "arith": args.arith,
                    "storage": args.storage, "l2": "inputs larger than L2 (%.2f GB volume, %.0f MB subset)"
                    % (4 * prob.nvox / 1e9, isz * prob.npix / 1e6), "parallelism": "independent volume per rank"},

@@ -172,9 +172,9 @@ static inline int pair_fast(const orc_projdata *d, float px, float py, float pz,
                             float hv, float rowsf, int32_t *iu, int32_t *iv)
 {
     const float *m = d->mvp;
-    float nu = fmaf(m[0], px, fmaf(m[1], py, m[3])) + m[2] * pz;
-    float nv = fmaf(m[4], px, fmaf(m[5], py, m[7])) + m[6] * pz;
-    float nw = fmaf(m[12], px, fmaf(m[13], py, m[15])) + m[14] * pz;
+    float nu = fmaf(m[1], py, fmaf(m[0], px, m[3]) + m[2] * pz);
+    float nv = fmaf(m[5], py, fmaf(m[4], px, m[7]) + m[6] * pz);
+    float nw = fmaf(m[13], py, fmaf(m[12], px, m[15]) + m[14] * pz);
     float rw = 1.0f / nw;
     float yu = fmaf(nu, rw, 0.5f);
     float yv = fmaf(nv, rw, hv);

@@ -29,8 +29,8 @@
  *                     p = idx*vx + o (mul, add); u = dot(c0,p)/dot(c3,p) with
  *                     dot = ((x*x'+y*y')+z*z')+w*w'; v likewise minus the line
  *                     offset; round half away from zero; saturating float->int.
- *   XPR_ARITH_FAST    p = fma(idx, vx, o); n_r = fma(c.x, px, fma(c.y, py, c.w))
- *                     + c.z*pz per row r in {0,1,3}; rw = 1/n_3 (IEEE);
+ *   XPR_ARITH_FAST    p = fma(idx, vx, o); n_r = fma(c.y, py, fma(c.x, px, c.w)
+ *                     + c.z*pz) per row r in {0,1,3}; rw = 1/n_3 (IEEE);
  *                     yu = fma(n_0, rw, 0.5); yv = fma(n_1, rw, 0.5 - line_offset);
  *                     in-bounds iff l <= yu < r and b <= yv < min(t, rows);
  *                     pixel = (floor(yu), floor(yv)).

@@ -40,14 +40,16 @@
 
 namespace xpr {
 
-constexpr int BX = 32;        // brick extent along x (one warp lane per x in z-lines)
-constexpr int BY = 8;         // brick extent along y (one warp per y)
-constexpr int BZ = 32;        // brick extent along z (forward)
-constexpr int NT = 256;       // threads per CTA
-constexpr int G = 4;          // projections whose tiles are in flight together
+constexpr int BX = 32;          // brick extent along x
+constexpr int BY = 8;           // forward brick extent along y (the column walked by a thread)
+constexpr int BZ = 32;          // forward brick extent along z
+constexpr int NT = 256;         // threads per CTA (8 warps)
+constexpr int G = 4;            // projections whose tiles are in flight together
 constexpr int TILE_CAP = 1024;  // pixels per shared-memory tile
-constexpr int VSTRIDE = 33;   // padded row stride of the brick value array (bank-conflict free both ways)
-constexpr int BWD_LZ = 16;    // backward line length along z
+constexpr int VSTRIDE = 33;     // padded row stride of the brick value array (bank-conflict free both ways)
+constexpr int BWD_BY = 16;      // backward column length along y
+constexpr int BWD_BZ = 8;       // backward brick extent along z (one warp per z)
+constexpr uint32_t kMagic = 0x4B000000u;  // float bits of 2^23: bits(fadd_rz(y, 2^23)) - kMagic = floor(y)
 
 enum Mode : int { kSkip = 0, kTile = 1, kDirect = 2 };
 
@@ -56,19 +58,23 @@ struct ProjMeta {
     float fu0, fu1, fv0, fv1;   // rectangle as floats (FAST bounds)
     int u0, u1, v0, v1;         // rectangle [u0,u1) x [v0,v1) in buffer coordinates
     int mode;
-    int orient_x;               // walk lines along x (ray closer to x than to z)
+    int orient_x;               // lanes across z (the ray is closer to x than to z)
+    int column;                 // u and w do not depend on y: a voxel column shares u, w, 1/w
     uint32_t img_base;          // image slot * det_w * rows
-    int tw;
+    int tw;                     // tile width
+    uint32_t TW;                // row pitch of the splat target (tile width or det_w)
+    uint32_t CT;                // target index = bits(v) * TW + bits(u) - CT (FAST)
+    uint32_t CS;                // target index = v * TW + u - CS (STRICT)
 };
 
 // --------------------------------------------------------------------------------------
 // per-projection metadata: one group of G entries, computed by warp 0
-// lane = g * 8 + corner
+// lane = g * 8 + corner of the brick [x0, x0+ex) x [y0, y0+ey) x [z0, z0+ez)
 // --------------------------------------------------------------------------------------
-template <bool LIST>
+template <bool LIST, bool GATHER>
 __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdata *__restrict__ pd,
                                              const LaunchArgs &a, int e0, int e_end, int bx0, int by0, int bz0,
-                                             int depth_z, int lane)
+                                             int ex, int ey, int ez, int lane)
 {
     const int g = lane >> 3, c = lane & 7;
     const int entry = e0 + g;
@@ -80,13 +86,13 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
         valid = pidx < a.n_pd && img < a.n_images;
     }
     const float *m = valid ? pd[pidx].mvp : pd[0].mvp;
-    float cu0 = __ldg(m + 0), cu1 = __ldg(m + 1), cu2 = __ldg(m + 2), cu3 = __ldg(m + 3);
-    float cv0 = __ldg(m + 4), cv1 = __ldg(m + 5), cv2 = __ldg(m + 6), cv3 = __ldg(m + 7);
-    float cw0 = __ldg(m + 12), cw1 = __ldg(m + 13), cw2 = __ldg(m + 14), cw3 = __ldg(m + 15);
+    const float cu0 = __ldg(m + 0), cu1 = __ldg(m + 1), cu2 = __ldg(m + 2), cu3 = __ldg(m + 3);
+    const float cv0 = __ldg(m + 4), cv1 = __ldg(m + 5), cv2 = __ldg(m + 6), cv3 = __ldg(m + 7);
+    const float cw0 = __ldg(m + 12), cw1 = __ldg(m + 13), cw2 = __ldg(m + 14), cw3 = __ldg(m + 15);
     // corner voxel centres of the brick (nominal extent; partial bricks are covered)
-    const int ix = a.vmin[0] + bx0 + ((c & 1) ? BX - 1 : 0);
-    const int iy = a.vmin[1] + by0 + ((c & 2) ? BY - 1 : 0);
-    const int iz = a.vmin[2] + bz0 + ((c & 4) ? depth_z - 1 : 0);
+    const int ix = a.vmin[0] + bx0 + ((c & 1) ? ex - 1 : 0);
+    const int iy = a.vmin[1] + by0 + ((c & 2) ? ey - 1 : 0);
+    const int iz = a.vmin[2] + bz0 + ((c & 4) ? ez - 1 : 0);
     const float px = __fmaf_rn((float)ix, a.voxel[0], a.origin[0]);
     const float py = __fmaf_rn((float)iy, a.voxel[1], a.origin[1]);
     const float pz = __fmaf_rn((float)iz, a.voxel[2], a.origin[2]);
@@ -121,10 +127,22 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
         M.u0 = l; M.u1 = r; M.v0 = b; M.v1 = t;
         M.fu0 = (float)l; M.fu1 = (float)r; M.fv0 = (float)b; M.fv1 = (float)t;
         const int area = (r - l) * (t - b);
-        M.mode = (!valid || r <= l || t <= b) ? kSkip : ((ok && area <= TILE_CAP) ? kTile : kDirect);
+        const int mode = (!valid || r <= l || t <= b) ? kSkip : ((ok && area <= TILE_CAP) ? kTile : kDirect);
+        M.mode = mode;
         M.tw = r - l;
         M.orient_x = fabsf(cw0) > fabsf(cw2);
+        M.column = (cu1 == 0.0f) && (cw1 == 0.0f);
         M.img_base = img * a.img_stride;
+        if (mode == kTile && !GATHER) {
+            const uint32_t tw = (uint32_t)(r - l);
+            M.TW = tw;
+            M.CS = (uint32_t)b * tw + (uint32_t)l;
+            M.CT = kMagic * (tw + 1u) + M.CS;
+        } else {
+            M.TW = a.det_w;
+            M.CS = 0u - M.img_base;
+            M.CT = kMagic * (a.det_w + 1u) - M.img_base;
+        }
         M.cu[0] = cu0; M.cu[1] = cu1; M.cu[2] = cu2; M.cu[3] = cu3;
         M.cv[0] = cv0; M.cv[1] = cv1; M.cv[2] = cv2; M.cv[3] = cv3;
         M.cw[0] = cw0; M.cw[1] = cw1; M.cw[2] = cw2; M.cw[3] = cw3;
@@ -132,116 +150,98 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
 }
 
 // --------------------------------------------------------------------------------------
-// one (voxel, projection) pair in each contract, given the line-invariant terms
+// positions and column-invariant numerators in each contract
 // --------------------------------------------------------------------------------------
-// FAST: n_r = A_r + B_r with A_r = fma(c.x, px, fma(c.y, py, c.w)), B_r = c.z * pz.
-// Returns in-rectangle; (iu_bits, iv_bits) are the float bits of 2^23 + pixel.
-__device__ __forceinline__ bool pair_fast(float nu, float nv, float nw, const ProjMeta &M, float hv,
-                                          uint32_t &iu_bits, uint32_t &iv_bits)
+template <int ARITH>
+__device__ __forceinline__ float pos(int idx, float vox, float org)
 {
-    const float rw = __frcp_rn(nw);
-    const float yu = __fmaf_rn(nu, rw, 0.5f);
-    const float yv = __fmaf_rn(nv, rw, hv);
-    const bool in = (yu >= M.fu0) && (yu < M.fu1) && (yv >= M.fv0) && (yv < M.fv1);
-    iu_bits = __float_as_uint(__fadd_rz(yu, 8388608.0f));
-    iv_bits = __float_as_uint(__fadd_rz(yv, 8388608.0f));
-    return in;
+    if (ARITH == kFast) return __fmaf_rn((float)idx, vox, org);
+    return __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)idx), vox), org);
 }
 
-// STRICT: u = n_u / n_w; v = n_v / n_w - off; round half away; saturating convert.
-__device__ __forceinline__ bool pair_strict(float nu, float nv, float nw, const ProjMeta &M, float off,
-                                            int &cu, int &cv)
+// FAST: C_r = fma(c.x, px, c.w) + c.z*pz, so that n_r = fma(c.y, py, C_r)
+__device__ __forceinline__ float col_fast(const float *c, float px, float pz)
 {
-    const float u = __fdiv_rn(nu, nw);
-    const float v = __fsub_rn(__fdiv_rn(nv, nw), off);
-    cu = __float2int_rz(roundf(u));
-    cv = __float2int_rz(roundf(v));
-    return (cu >= M.u0) && (cu < M.u1) && (cv >= M.v0) && (cv < M.v1);
+    return __fadd_rn(__fmaf_rn(c[0], px, c[3]), __fmul_rn(c[2], pz));
 }
 
-// Line walker: calls f(k, in, tile_index, global_index) for the voxels k = 0..LEN-1 of
-// this thread's line.  ORX: walk along x (lane = z), else along z (lane = x).
-template <int ARITH, bool ORX, int LEN, typename F>
-__device__ __forceinline__ void walk_line(const ProjMeta &M, const LaunchArgs &a, int ax, int ay, int az, F &&f)
+// STRICT: n_r = ((c.x*px + c.y*py) + c.z*pz) + c.w
+__device__ __forceinline__ float num_strict(const float *c, float px, float py, float pz)
 {
-    const float vx = a.voxel[0], vy = a.voxel[1], vz = a.voxel[2];
-    const float ox = a.origin[0], oy = a.origin[1], oz = a.origin[2];
-    const uint32_t W = a.det_w;
-    const uint32_t tw = (uint32_t)M.tw;
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c[0], px), __fmul_rn(c[1], py)), __fmul_rn(c[2], pz)), c[3]);
+}
+
+// Column walker.  For a voxel column (ax, az) and the y-positions py[0..LEN), calls
+// f(k, in, idx) with idx = index in the projection's splat target (tile or global
+// image, see ProjMeta::TW / CT / CS).  Untilted projections (M.column) hoist u, w and
+// 1/w out of the column; the others evaluate the full contract per voxel.
+template <int ARITH, int LEN, typename F>
+__device__ __forceinline__ void walk_column(const ProjMeta &M, const LaunchArgs &a, int ax, int az,
+                                            const float (&py)[LEN], F &&f)
+{
+    const float px = pos<ARITH>(ax, a.voxel[0], a.origin[0]);
+    const float pz = pos<ARITH>(az, a.voxel[2], a.origin[2]);
+    const uint32_t TW = M.TW;
     if (ARITH == kFast) {
-        const float py = __fmaf_rn((float)ay, vy, oy);
-        // tile index = (iv - v0) * tw + (iu - u0) with iu = iu_bits - 0x4B000000
-        const uint32_t ct = 0x4B000000u * (tw + 1u) + (uint32_t)M.v0 * tw + (uint32_t)M.u0;
-        const uint32_t cg = 0x4B000000u * (W + 1u) - M.img_base;
-        if (!ORX) {
-            const float px = __fmaf_rn((float)ax, vx, ox);
-            const float Au = __fmaf_rn(M.cu[0], px, __fmaf_rn(M.cu[1], py, M.cu[3]));
-            const float Av = __fmaf_rn(M.cv[0], px, __fmaf_rn(M.cv[1], py, M.cv[3]));
-            const float Aw = __fmaf_rn(M.cw[0], px, __fmaf_rn(M.cw[1], py, M.cw[3]));
-            const float fz0 = (float)az;
+        const float Cu = col_fast(M.cu, px, pz), Cv = col_fast(M.cv, px, pz), Cw = col_fast(M.cw, px, pz);
+        const float hv = a.half_minus_off;
+        if (M.column) {
+            const float rw = __frcp_rn(Cw);
+            const float yu = __fmaf_rn(Cu, rw, 0.5f);
+            const bool in_u = (yu >= M.fu0) && (yu < M.fu1);
+            if (!__any_sync(0xffffffffu, in_u)) return;
+            const uint32_t K = __float_as_uint(__fadd_rz(yu, 8388608.0f)) - M.CT;
+            const float cvy = M.cv[1];
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float pz = __fmaf_rn(__fadd_rn(fz0, (float)k), vz, oz);
-                const float nu = __fadd_rn(Au, __fmul_rn(M.cu[2], pz));
-                const float nv = __fadd_rn(Av, __fmul_rn(M.cv[2], pz));
-                const float nw = __fadd_rn(Aw, __fmul_rn(M.cw[2], pz));
-                uint32_t ub, vb;
-                const bool in = pair_fast(nu, nv, nw, M, a.half_minus_off, ub, vb);
-                f(k, in, vb * tw + ub - ct, vb * W + ub - cg);
+                const float yv = __fmaf_rn(__fmaf_rn(cvy, py[k], Cv), rw, hv);
+                const bool in = in_u && (yv >= M.fv0) && (yv < M.fv1);
+                f(k, in, __float_as_uint(__fadd_rz(yv, 8388608.0f)) * TW + K);
             }
         } else {
-            const float pz = __fmaf_rn((float)az, vz, oz);
-            const float Ku = __fmaf_rn(M.cu[1], py, M.cu[3]);
-            const float Kv = __fmaf_rn(M.cv[1], py, M.cv[3]);
-            const float Kw = __fmaf_rn(M.cw[1], py, M.cw[3]);
-            const float Bu = __fmul_rn(M.cu[2], pz);
-            const float Bv = __fmul_rn(M.cv[2], pz);
-            const float Bw = __fmul_rn(M.cw[2], pz);
-            const float fx0 = (float)ax;
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float px = __fmaf_rn(__fadd_rn(fx0, (float)k), vx, ox);
-                const float nu = __fadd_rn(__fmaf_rn(M.cu[0], px, Ku), Bu);
-                const float nv = __fadd_rn(__fmaf_rn(M.cv[0], px, Kv), Bv);
-                const float nw = __fadd_rn(__fmaf_rn(M.cw[0], px, Kw), Bw);
-                uint32_t ub, vb;
-                const bool in = pair_fast(nu, nv, nw, M, a.half_minus_off, ub, vb);
-                f(k, in, vb * tw + ub - ct, vb * W + ub - cg);
+                const float nu = __fmaf_rn(M.cu[1], py[k], Cu);
+                const float nv = __fmaf_rn(M.cv[1], py[k], Cv);
+                const float nw = __fmaf_rn(M.cw[1], py[k], Cw);
+                const float rw = __frcp_rn(nw);
+                const float yu = __fmaf_rn(nu, rw, 0.5f);
+                const float yv = __fmaf_rn(nv, rw, hv);
+                const bool in = (yu >= M.fu0) && (yu < M.fu1) && (yv >= M.fv0) && (yv < M.fv1);
+                f(k, in, __float_as_uint(__fadd_rz(yv, 8388608.0f)) * TW +
+                             __float_as_uint(__fadd_rz(yu, 8388608.0f)) - M.CT);
             }
         }
     } else {
-        // STRICT: p = float(idx) * vx + o;  n = ((c.x*px + c.y*py) + c.z*pz) + c.w
-        const float py = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)ay), vy), oy);
-        const uint32_t ct = (uint32_t)M.v0 * tw + (uint32_t)M.u0;
-        if (!ORX) {
-            const float px = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)ax), vx), ox);
-            const float Pu = __fadd_rn(__fmul_rn(M.cu[0], px), __fmul_rn(M.cu[1], py));
-            const float Pv = __fadd_rn(__fmul_rn(M.cv[0], px), __fmul_rn(M.cv[1], py));
-            const float Pw = __fadd_rn(__fmul_rn(M.cw[0], px), __fmul_rn(M.cw[1], py));
+        const float off = a.row_off_f;
+        if (M.column) {
+            // c.y == 0 in the u and w rows: c.y*py is a zero for every voxel of the column,
+            // so n_u and n_w (up to the sign of a zero, which never changes a pixel) are
+            // column invariants
+            const float nu = num_strict(M.cu, px, 0.0f, pz);
+            const float nw = num_strict(M.cw, px, 0.0f, pz);
+            const int iu = __float2int_rz(roundf(__fdiv_rn(nu, nw)));
+            const bool in_u = (iu >= M.u0) && (iu < M.u1);
+            if (!__any_sync(0xffffffffu, in_u)) return;
+            const uint32_t K = (uint32_t)iu - M.CS;
+            const float Pv = __fmul_rn(M.cv[0], px), Rv = __fmul_rn(M.cv[2], pz);
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float pz = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)(az + k)), vz), oz);
-                const float nu = __fadd_rn(__fadd_rn(Pu, __fmul_rn(M.cu[2], pz)), M.cu[3]);
-                const float nv = __fadd_rn(__fadd_rn(Pv, __fmul_rn(M.cv[2], pz)), M.cv[3]);
-                const float nw = __fadd_rn(__fadd_rn(Pw, __fmul_rn(M.cw[2], pz)), M.cw[3]);
-                int cu, cv;
-                const bool in = pair_strict(nu, nv, nw, M, a.row_off_f, cu, cv);
-                f(k, in, (uint32_t)cv * tw + (uint32_t)cu - ct, M.img_base + (uint32_t)cv * W + (uint32_t)cu);
+                const float nv = __fadd_rn(__fadd_rn(__fadd_rn(Pv, __fmul_rn(M.cv[1], py[k])), Rv), M.cv[3]);
+                const int iv = __float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off)));
+                const bool in = in_u && (iv >= M.v0) && (iv < M.v1);
+                f(k, in, (uint32_t)iv * TW + K);
             }
         } else {
-            const float pz = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)az), vz), oz);
-            const float Qu = __fmul_rn(M.cu[1], py), Ru = __fmul_rn(M.cu[2], pz);
-            const float Qv = __fmul_rn(M.cv[1], py), Rv = __fmul_rn(M.cv[2], pz);
-            const float Qw = __fmul_rn(M.cw[1], py), Rw = __fmul_rn(M.cw[2], pz);
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float px = __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)(ax + k)), vx), ox);
-                const float nu = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(M.cu[0], px), Qu), Ru), M.cu[3]);
-                const float nv = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(M.cv[0], px), Qv), Rv), M.cv[3]);
-                const float nw = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(M.cw[0], px), Qw), Rw), M.cw[3]);
-                int cu, cv;
-                const bool in = pair_strict(nu, nv, nw, M, a.row_off_f, cu, cv);
-                f(k, in, (uint32_t)cv * tw + (uint32_t)cu - ct, M.img_base + (uint32_t)cv * W + (uint32_t)cu);
+                const float nu = num_strict(M.cu, px, py[k], pz);
+                const float nv = num_strict(M.cv, px, py[k], pz);
+                const float nw = num_strict(M.cw, px, py[k], pz);
+                const int iu = __float2int_rz(roundf(__fdiv_rn(nu, nw)));
+                const int iv = __float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off)));
+                const bool in = (iu >= M.u0) && (iu < M.u1) && (iv >= M.v0) && (iv < M.v1);
+                f(k, in, (uint32_t)iv * TW + (uint32_t)iu - M.CS);
             }
         }
     }
@@ -253,12 +253,12 @@ __device__ __forceinline__ void walk_line(const ProjMeta &M, const LaunchArgs &a
 constexpr size_t kFwdSmem = (size_t)(BY * BZ * VSTRIDE + G * TILE_CAP) * sizeof(uint32_t);
 
 template <int ARITH, bool LIST>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, 4)
     k_forward_tiled(const float *__restrict__ vol, uint32_t *__restrict__ sum, const xpr_projdata *__restrict__ pd,
                     const LaunchArgs a, int bricks_x, int bricks_z)
 {
     extern __shared__ uint32_t smem[];
-    uint32_t *s_val = smem;                        // [BY][BZ][VSTRIDE]
+    uint32_t *s_val = smem;                        // [BY][BZ][VSTRIDE] fixed-point values
     uint32_t *s_tile = smem + BY * BZ * VSTRIDE;   // [G][TILE_CAP]
     __shared__ ProjMeta s_meta[G];
 
@@ -283,12 +283,15 @@ __global__ void __launch_bounds__(NT, 3)
     for (int i = threadIdx.x; i < G * TILE_CAP; i += NT) s_tile[i] = 0u;
     if (!__syncthreads_or(any)) return;   // an all-zero brick adds nothing
 
+    float py[BY];
+#pragma unroll
+    for (int k = 0; k < BY; ++k) py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
+
     const int e_begin = blockIdx.y * (int)a.per_split;
     const int e_end = min((int)a.n_entries, e_begin + (int)a.per_split);
-    const int ay = a.vmin[1] + y0 + warp;
 
     for (int e0 = e_begin; e0 < e_end; e0 += G) {
-        if (warp == 0) compute_meta<LIST>(s_meta, pd, a, e0, e_end, x0, y0, z0, BZ, lane);
+        if (warp == 0) compute_meta<LIST, false>(s_meta, pd, a, e0, e_end, x0, y0, z0, BX, BY, BZ, lane);
         __syncthreads();
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
@@ -296,35 +299,23 @@ __global__ void __launch_bounds__(NT, 3)
             const int mode = M.mode;
             if (mode == kSkip) continue;
             uint32_t *tile = s_tile + g * TILE_CAP;
-            uint32_t acc = 0u, prev = 0xffffffffu;
-            auto splat = [&](int k, bool in, uint32_t tidx, uint32_t gidx, uint32_t val) {
-                const uint32_t idx = (mode == kTile) ? tidx : gidx;
-                if (in && idx != prev) {
-                    if (acc) {
-                        if (mode == kTile) atomicAdd(&tile[prev], acc);
-                        else atomicAdd(&sum[prev], acc);
+            const bool orx = M.orient_x;
+            // 4 columns per thread; lanes run across the ray so a warp hits distinct pixels
+#pragma unroll 1
+            for (int j = 0; j < 4; ++j) {
+                const int cx = orx ? warp + 8 * j : lane;
+                const int cz = orx ? lane : warp + 8 * j;
+                const uint32_t *vals = s_val + cz * VSTRIDE + cx;
+                auto splat = [&](int k, bool in, uint32_t idx) {
+                    if (in) {
+                        const uint32_t v = vals[k * BZ * VSTRIDE];
+                        if (v) {
+                            if (mode == kTile) atomicAdd(&tile[idx], v);
+                            else atomicAdd(&sum[idx], v);
+                        }
                     }
-                    acc = 0u;
-                    prev = idx;
-                }
-                acc += in ? val : 0u;
-            };
-            if (M.orient_x) {
-                // lane = z, walk x
-                const uint32_t *row = s_val + (warp * BZ + lane) * VSTRIDE;
-                walk_line<ARITH, true, BX>(M, a, a.vmin[0] + x0, ay, a.vmin[2] + z0 + lane,
-                                           [&](int k, bool in, uint32_t t, uint32_t gi) { splat(k, in, t, gi, row[k]); });
-            } else {
-                // lane = x, walk z
-                const uint32_t *col = s_val + warp * BZ * VSTRIDE + lane;
-                walk_line<ARITH, false, BZ>(M, a, a.vmin[0] + x0 + lane, ay, a.vmin[2] + z0,
-                                            [&](int k, bool in, uint32_t t, uint32_t gi) {
-                                                splat(k, in, t, gi, col[k * VSTRIDE]);
-                                            });
-            }
-            if (acc) {
-                if (mode == kTile) atomicAdd(&tile[prev], acc);
-                else atomicAdd(&sum[prev], acc);
+                };
+                walk_column<ARITH, BY>(M, a, a.vmin[0] + x0 + cx, a.vmin[2] + z0 + cz, py, splat);
             }
         }
         __syncthreads();
@@ -385,9 +376,9 @@ __global__ void k_pad_items(float *vol, uint32_t *sum, const void *ratio, const 
         int iu, iv;
         bool in;
         if (ARITH == kFast) {
-            const float nu = __fadd_rn(__fmaf_rn(m[0], px, __fmaf_rn(m[1], py, m[3])), __fmul_rn(m[2], pz));
-            const float nv = __fadd_rn(__fmaf_rn(m[4], px, __fmaf_rn(m[5], py, m[7])), __fmul_rn(m[6], pz));
-            const float nw = __fadd_rn(__fmaf_rn(m[12], px, __fmaf_rn(m[13], py, m[15])), __fmul_rn(m[14], pz));
+            const float nu = __fmaf_rn(m[1], py, col_fast(m + 0, px, pz));
+            const float nv = __fmaf_rn(m[5], py, col_fast(m + 4, px, pz));
+            const float nw = __fmaf_rn(m[13], py, col_fast(m + 12, px, pz));
             const float rw = __frcp_rn(nw);
             const float yu = __fmaf_rn(nu, rw, 0.5f), yv = __fmaf_rn(nv, rw, a.half_minus_off);
             in = yu >= (float)l && yu < (float)r && yv >= (float)bb && yv < (float)t;
@@ -430,7 +421,7 @@ __device__ __forceinline__ float load_ratio(const void *ratio, uint32_t i)
 }
 
 template <int ARITH, bool LIST, bool NANSKIP, int DT>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, 3)
     k_backward_tiled(float *__restrict__ vol, const void *__restrict__ ratio, const xpr_projdata *__restrict__ pd,
                      const LaunchArgs a, int bricks_x, int bricks_z)
 {
@@ -441,24 +432,31 @@ __global__ void __launch_bounds__(NT, 2)
     b /= bricks_x;
     const int bzi = b % bricks_z;
     const int byi = b / bricks_z;
-    const int x0 = bxi * BX, y0 = byi * BY, z0 = bzi * BWD_LZ;
-    const int ax = a.vmin[0] + x0 + lane, ay = a.vmin[1] + y0 + warp, az = a.vmin[2] + z0;
+    const int x0 = bxi * BX, y0 = byi * BWD_BY, z0 = bzi * BWD_BZ;
+    // thread = the voxel column (x0 + lane, z0 + warp), layers y0 .. y0 + BWD_BY
+    const int ax = a.vmin[0] + x0 + lane, az = a.vmin[2] + z0 + warp;
 
-    float s[BWD_LZ];
-    uint32_t n[BWD_LZ];
+    float py[BWD_BY], s[BWD_BY];
+    uint32_t n[BWD_BY];
 #pragma unroll
-    for (int k = 0; k < BWD_LZ; ++k) { s[k] = 0.0f; n[k] = 0u; }
+    for (int k = 0; k < BWD_BY; ++k) {
+        py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
+        s[k] = 0.0f;
+        n[k] = 0u;
+    }
 
     for (int e0 = 0; e0 < (int)a.n_entries; e0 += G) {
-        if (warp == 0) compute_meta<LIST>(s_meta, pd, a, e0, (int)a.n_entries, x0, y0, z0, BWD_LZ, lane);
+        if (warp == 0)
+            compute_meta<LIST, true>(s_meta, pd, a, e0, (int)a.n_entries, x0, y0, z0, BX, BWD_BY, BWD_BZ, lane);
         __syncthreads();
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
             const ProjMeta &M = s_meta[g];
             if (M.mode == kSkip) continue;
-            walk_line<ARITH, false, BWD_LZ>(M, a, ax, ay, az, [&](int k, bool in, uint32_t, uint32_t gi) {
+            // gathers index the whole image (compute_meta<.., GATHER = true>)
+            walk_column<ARITH, BWD_BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
                 if (in) {
-                    const float r = load_ratio<DT>(ratio, gi);
+                    const float r = load_ratio<DT>(ratio, idx);
                     if (!NANSKIP || r == r) {
                         s[k] = __fadd_rn(s[k], r);
                         n[k] += 1u;
@@ -469,12 +467,12 @@ __global__ void __launch_bounds__(NT, 2)
         __syncthreads();
     }
     const int sx = a.size[0], sy = a.size[1], sz = a.size[2];
-    const int x = x0 + lane, y = y0 + warp;
-    if (x >= sx || y >= sy) return;
+    const int x = x0 + lane, z = z0 + warp;
+    if (x >= sx || z >= sz) return;
 #pragma unroll
-    for (int k = 0; k < BWD_LZ; ++k) {
-        const int z = z0 + k;
-        if (z < sz) {
+    for (int k = 0; k < BWD_BY; ++k) {
+        const int y = y0 + k;
+        if (y < sy) {
             float *p = vol + ((size_t)y * sz + z) * sx + x;
             *p = __fmul_rn(*p, p_expf(__fdiv_rn(s[k], __uint2float_rn(n[k]))));
         }
@@ -746,7 +744,8 @@ cudaError_t launch_backward(float *vol, const void *ratio, int dt, const xpr_pro
                             int arith, int compat_pad, int nan_skip, const DeviceInfo &dev, cudaStream_t s)
 {
     (void)dev;
-    const int bx = (a.size[0] + BX - 1) / BX, by = (a.size[1] + BY - 1) / BY, bz = (a.size[2] + BWD_LZ - 1) / BWD_LZ;
+    const int bx = (a.size[0] + BX - 1) / BX, by = (a.size[1] + BWD_BY - 1) / BWD_BY,
+              bz = (a.size[2] + BWD_BZ - 1) / BWD_BZ;
     const uint64_t bricks = (uint64_t)bx * by * bz;
     const bool list = a.list_mvp != nullptr;
     dim3 grid((unsigned)bricks);
