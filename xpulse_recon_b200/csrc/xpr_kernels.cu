@@ -306,16 +306,18 @@ __global__ void __launch_bounds__(NT, 4)
                 const int cx = orx ? warp + 8 * j : lane;
                 const int cz = orx ? lane : warp + 8 * j;
                 const uint32_t *vals = s_val + cz * VSTRIDE + cx;
-                auto splat = [&](int k, bool in, uint32_t idx) {
-                    if (in) {
+                const int ax = a.vmin[0] + x0 + cx, az = a.vmin[2] + z0 + cz;
+                if (mode == kTile) {
+                    walk_column<ARITH, BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
                         const uint32_t v = vals[k * BZ * VSTRIDE];
-                        if (v) {
-                            if (mode == kTile) atomicAdd(&tile[idx], v);
-                            else atomicAdd(&sum[idx], v);
-                        }
-                    }
-                };
-                walk_column<ARITH, BY>(M, a, a.vmin[0] + x0 + cx, a.vmin[2] + z0 + cz, py, splat);
+                        if (in & (v != 0u)) atomicAdd(&tile[idx], v);
+                    });
+                } else {
+                    walk_column<ARITH, BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
+                        const uint32_t v = vals[k * BZ * VSTRIDE];
+                        if (in & (v != 0u)) atomicAdd(&sum[idx], v);
+                    });
+                }
             }
         }
         __syncthreads();
@@ -435,15 +437,17 @@ __global__ void __launch_bounds__(NT, 3)
     const int x0 = bxi * BX, y0 = byi * BWD_BY, z0 = bzi * BWD_BZ;
     // thread = the voxel column (x0 + lane, z0 + warp), layers y0 .. y0 + BWD_BY
     const int ax = a.vmin[0] + x0 + lane, az = a.vmin[2] + z0 + warp;
+    constexpr int HB = BWD_BY / 2;  // gathers are issued in two batches of HB
 
     float py[BWD_BY], s[BWD_BY];
-    uint32_t n[BWD_BY];
+    uint32_t n2[HB];  // in-bounds counts, two 16-bit halves per word (k even: low, odd: high)
 #pragma unroll
     for (int k = 0; k < BWD_BY; ++k) {
         py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
         s[k] = 0.0f;
-        n[k] = 0u;
     }
+#pragma unroll
+    for (int k = 0; k < HB; ++k) n2[k] = 0u;
 
     for (int e0 = 0; e0 < (int)a.n_entries; e0 += G) {
         if (warp == 0)
@@ -453,16 +457,34 @@ __global__ void __launch_bounds__(NT, 3)
         for (int g = 0; g < G; ++g) {
             const ProjMeta &M = s_meta[g];
             if (M.mode == kSkip) continue;
-            // gathers index the whole image (compute_meta<.., GATHER = true>)
-            walk_column<ARITH, BWD_BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
-                if (in) {
-                    const float r = load_ratio<DT>(ratio, idx);
-                    if (!NANSKIP || r == r) {
-                        s[k] = __fadd_rn(s[k], r);
-                        n[k] += 1u;
+            // gathers index the whole image (compute_meta<.., GATHER = true>); the column's
+            // indices are computed first so all its loads are in flight together
+            uint32_t idx[BWD_BY];
+            uint32_t inmask = 0u;
+            walk_column<ARITH, BWD_BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t i) {
+                idx[k] = i;
+                inmask |= (in ? 1u : 0u) << k;
+            });
+            if (inmask == 0u) continue;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float r[HB];
+#pragma unroll
+                for (int q = 0; q < HB; ++q) {
+                    const int k = h * HB + q;
+                    r[q] = 0.0f;
+                    if (inmask & (1u << k)) r[q] = load_ratio<DT>(ratio, idx[k]);
+                }
+#pragma unroll
+                for (int q = 0; q < HB; ++q) {
+                    const int k = h * HB + q;
+                    const bool take = ((inmask >> k) & 1u) && (!NANSKIP || r[q] == r[q]);
+                    if (take) {
+                        s[k] = __fadd_rn(s[k], r[q]);
+                        n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
                     }
                 }
-            });
+            }
         }
         __syncthreads();
     }
@@ -473,8 +495,9 @@ __global__ void __launch_bounds__(NT, 3)
     for (int k = 0; k < BWD_BY; ++k) {
         const int y = y0 + k;
         if (y < sy) {
+            const uint32_t cnt = (k & 1) ? (n2[k >> 1] >> 16) : (n2[k >> 1] & 0xffffu);
             float *p = vol + ((size_t)y * sz + z) * sx + x;
-            *p = __fmul_rn(*p, p_expf(__fdiv_rn(s[k], __uint2float_rn(n[k]))));
+            *p = __fmul_rn(*p, p_expf(__fdiv_rn(s[k], __uint2float_rn(cnt))));
         }
     }
 }
@@ -651,6 +674,7 @@ const char *make_launch_args(const xpr_launch *L, uint32_t n_pd, LaunchArgs *a)
         a->n_images = L->n_angles;
     }
     if ((uint64_t)a->img_stride * a->n_images >= (1ull << 32)) return "detector buffer exceeds 2^32 elements";
+    if (a->n_entries > 65535u) return "more than 65535 (angle, module) entries in one launch";
     const uint64_t nvox = (uint64_t)a->size[0] * a->size[1] * a->size[2];
     if (nvox + 64 >= (1ull << 40)) return "volume box too large";
     a->per_split = a->n_entries;
