@@ -172,12 +172,12 @@ static inline int pair_fast(const orc_projdata *d, float px, float py, float pz,
                             float hv, float rowsf, int32_t *iu, int32_t *iv)
 {
     const float *m = d->mvp;
-    float nu = fmaf(m[1], py, fmaf(m[0], px, m[3]) + m[2] * pz);
-    float nv = fmaf(m[5], py, fmaf(m[4], px, m[7]) + m[6] * pz);
-    float nw = fmaf(m[13], py, fmaf(m[12], px, m[15]) + m[14] * pz);
-    float rw = 1.0f / nw;
-    float yu = fmaf(nu, rw, 0.5f);
-    float yv = fmaf(nv, rw, hv);
+    float cu = fmaf(m[0], px, m[3]) + m[2] * pz;
+    float cv = fmaf(m[4], px, m[7]) + m[6] * pz;
+    float cw = fmaf(m[12], px, m[15]) + m[14] * pz;
+    float rw = 1.0f / fmaf(m[13], py, cw);
+    float yu = fmaf(py, m[1] * rw, fmaf(cu, rw, 0.5f));
+    float yv = fmaf(py, m[5] * rw, fmaf(cv, rw, hv));
     int in = (yu >= d->vp[0]) && (yu < d->vp[1]) && (yv >= d->vp[2]) && (yv < d->vp[3]) &&
              (yv < rowsf);
     if (in) {

@@ -20,7 +20,7 @@
  *
  * Parity pin: the kernel restatements (arith = XPR_ARITH_STRICT) are checked
  * bit-for-bit against the reference's own OpenCL kernel sources compiled for
- * the CPU (oracle/_ref, built by oracle/build_ref.py).  The geometry depends on
+ * the CPU (oracle/_ref, built by oracle/build.py).  The geometry depends on
  * glm, an un-vendored submodule with no pinned commit: it is restated from
  * glm's published semantics and its parity is unpinned at that boundary.
  *
@@ -29,11 +29,13 @@
  *                     p = idx*vx + o (mul, add); u = dot(c0,p)/dot(c3,p) with
  *                     dot = ((x*x'+y*y')+z*z')+w*w'; v likewise minus the line
  *                     offset; round half away from zero; saturating float->int.
- *   XPR_ARITH_FAST    p = fma(idx, vx, o); n_r = fma(c.y, py, fma(c.x, px, c.w)
- *                     + c.z*pz) per row r in {0,1,3}; rw = 1/n_3 (IEEE);
- *                     yu = fma(n_0, rw, 0.5); yv = fma(n_1, rw, 0.5 - line_offset);
+ *   XPR_ARITH_FAST    p = fma(idx, vx, o); C_r = fma(c_r.x, px, c_r.w) + c_r.z*pz
+ *                     for the rows r = u, v, w; rw = 1/fma(c_w.y, py, C_w) (IEEE);
+ *                     yu = fma(py, c_u.y*rw, fma(C_u, rw, 0.5));
+ *                     yv = fma(py, c_v.y*rw, fma(C_v, rw, 0.5 - line_offset));
  *                     in-bounds iff l <= yu < r and b <= yv < min(t, rows);
- *                     pixel = (floor(yu), floor(yv)).
+ *                     pixel = (floor(yu), floor(yv)).  Along a voxel column of an
+ *                     untilted detector (c_u.y = c_w.y = 0) only yv varies, by one fma.
  * exp/log are this project's own portable single-precision functions (Cody-Waite
  * reduction + Taylor polynomial; atanh series), identical on CPU and GPU.
  */

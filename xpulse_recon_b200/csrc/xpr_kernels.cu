@@ -53,18 +53,17 @@ constexpr uint32_t kMagic = 0x4B000000u;  // float bits of 2^23: bits(fadd_rz(y,
 
 enum Mode : int { kSkip = 0, kTile = 1, kDirect = 2 };
 
-struct ProjMeta {
-    float cu[4], cv[4], cw[4];  // matrix rows for u, v, w (glm columns c0, c1, c3)
-    float fu0, fu1, fv0, fv1;   // rectangle as floats (FAST bounds)
-    int u0, u1, v0, v1;         // rectangle [u0,u1) x [v0,v1) in buffer coordinates
-    int mode;
-    int orient_x;               // lanes across z (the ray is closer to x than to z)
-    int column;                 // u and w do not depend on y: a voxel column shares u, w, 1/w
-    uint32_t img_base;          // image slot * det_w * rows
-    int tw;                     // tile width
-    uint32_t TW;                // row pitch of the splat target (tile width or det_w)
-    uint32_t CT;                // target index = bits(v) * TW + bits(u) - CT (FAST)
-    uint32_t CS;                // target index = v * TW + u - CS (STRICT)
+// Per-projection constants of one (brick, projection) pair, read by every thread as
+// 16-byte vectors.  Rectangle [u0, u1) x [v0, v1) in buffer coordinates; a pixel
+// (iu, iv) inside it goes to target index (iv - v0) * pitch + (iu - u0) + off, where
+// the target is the shared-memory tile (pitch = tile width, off = 0) or the whole
+// detector buffer (pitch = det_w, off = img_base + v0 * det_w + u0).
+struct __align__(16) ProjMeta {
+    float4 cu, cv, cw;                    // matrix rows for u, v, w (glm columns c0, c1, c3)
+    uint4 fast;                           // {kMagic + u0, u1 - u0, kMagic + v0, v1 - v0}
+    int4 rect;                            // {u0, u1 - u0, v0, v1 - v0}
+    uint4 tgt;                            // {pitch, off, img_base, tile width}
+    int4 flags;                           // {mode, lanes across z, column, v1 - v0 (rows)}
 };
 
 // --------------------------------------------------------------------------------------
@@ -124,28 +123,19 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
             b = max(b, (int)floorf(vmn) - 2);
             t = min(t, (int)ceilf(vmx) + 3);
         }
-        M.u0 = l; M.u1 = r; M.v0 = b; M.v1 = t;
-        M.fu0 = (float)l; M.fu1 = (float)r; M.fv0 = (float)b; M.fv1 = (float)t;
         const int area = (r - l) * (t - b);
         const int mode = (!valid || r <= l || t <= b) ? kSkip : ((ok && area <= TILE_CAP) ? kTile : kDirect);
-        M.mode = mode;
-        M.tw = r - l;
-        M.orient_x = fabsf(cw0) > fabsf(cw2);
-        M.column = (cu1 == 0.0f) && (cw1 == 0.0f);
-        M.img_base = img * a.img_stride;
-        if (mode == kTile && !GATHER) {
-            const uint32_t tw = (uint32_t)(r - l);
-            M.TW = tw;
-            M.CS = (uint32_t)b * tw + (uint32_t)l;
-            M.CT = kMagic * (tw + 1u) + M.CS;
-        } else {
-            M.TW = a.det_w;
-            M.CS = 0u - M.img_base;
-            M.CT = kMagic * (a.det_w + 1u) - M.img_base;
-        }
-        M.cu[0] = cu0; M.cu[1] = cu1; M.cu[2] = cu2; M.cu[3] = cu3;
-        M.cv[0] = cv0; M.cv[1] = cv1; M.cv[2] = cv2; M.cv[3] = cv3;
-        M.cw[0] = cw0; M.cw[1] = cw1; M.cw[2] = cw2; M.cw[3] = cw3;
+        const uint32_t img_base = img * a.img_stride;
+        const bool tile = (mode == kTile) && !GATHER;
+        const uint32_t pitch = tile ? (uint32_t)(r - l) : a.det_w;
+        const uint32_t off = tile ? 0u : img_base + (uint32_t)b * a.det_w + (uint32_t)l;
+        M.cu = make_float4(cu0, cu1, cu2, cu3);
+        M.cv = make_float4(cv0, cv1, cv2, cv3);
+        M.cw = make_float4(cw0, cw1, cw2, cw3);
+        M.fast = make_uint4(kMagic + (uint32_t)l, (uint32_t)(r - l), kMagic + (uint32_t)b, (uint32_t)(t - b));
+        M.rect = make_int4(l, r - l, b, t - b);
+        M.tgt = make_uint4(pitch, off, img_base, (uint32_t)(r - l));
+        M.flags = make_int4(mode, fabsf(cw0) > fabsf(cw2), (cu1 == 0.0f) && (cw1 == 0.0f), t - b);
     }
 }
 
@@ -159,92 +149,98 @@ __device__ __forceinline__ float pos(int idx, float vox, float org)
     return __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)idx), vox), org);
 }
 
-// FAST: C_r = fma(c.x, px, c.w) + c.z*pz, so that n_r = fma(c.y, py, C_r)
-__device__ __forceinline__ float col_fast(const float *c, float px, float pz)
+// FAST: C = fma(c.x, px, c.w) + c.z*pz
+__device__ __forceinline__ float col_fast(float4 c, float px, float pz)
 {
-    return __fadd_rn(__fmaf_rn(c[0], px, c[3]), __fmul_rn(c[2], pz));
+    return __fadd_rn(__fmaf_rn(c.x, px, c.w), __fmul_rn(c.z, pz));
 }
 
-// STRICT: n_r = ((c.x*px + c.y*py) + c.z*pz) + c.w
-__device__ __forceinline__ float num_strict(const float *c, float px, float py, float pz)
+// STRICT: n = ((c.x*px + c.y*py) + c.z*pz) + c.w
+__device__ __forceinline__ float num_strict(float4 c, float px, float py, float pz)
 {
-    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c[0], px), __fmul_rn(c[1], py)), __fmul_rn(c[2], pz)), c[3]);
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.x, px), __fmul_rn(c.y, py)), __fmul_rn(c.z, pz)), c.w);
 }
 
-// Column walker.  For a voxel column (ax, az) and the y-positions py[0..LEN), calls
-// f(k, in, idx) with idx = index in the projection's splat target (tile or global
-// image, see ProjMeta::TW / CT / CS).  Untilted projections (M.column) hoist u, w and
-// 1/w out of the column; the others evaluate the full contract per voxel.
+// bits of fadd_rz(y, 2^23) minus `base`: for 0 <= y < 2^22 this is floor(y) - (base - kMagic);
+// every other y (negative, >= 2^22, inf, NaN) gives a value >= 2^23 as unsigned, so
+// "d < range" with range <= 2^22 is exactly "base' <= y < base' + range".
+__device__ __forceinline__ uint32_t fdist(float y, uint32_t base)
+{
+    return __float_as_uint(__fadd_rz(y, 8388608.0f)) - base;
+}
+
+// Column walker.  For the voxel column (ax, az) and y-positions py[0..LEN), calls
+// f(k, in, idx) with idx the target index of ProjMeta.  Untilted projections
+// (flags.z) hoist u, w and 1/w out of the column; the others evaluate the full
+// contract per voxel.  Returns false, without calling f, when no column of the
+// warp meets the projection's u range.
 template <int ARITH, int LEN, typename F>
-__device__ __forceinline__ void walk_column(const ProjMeta &M, const LaunchArgs &a, int ax, int az,
+__device__ __forceinline__ bool walk_column(const ProjMeta &M, const LaunchArgs &a, int ax, int az,
                                             const float (&py)[LEN], F &&f)
 {
+    const float4 cu = M.cu, cv = M.cv, cw = M.cw;
+    const uint4 tgt = M.tgt;
     const float px = pos<ARITH>(ax, a.voxel[0], a.origin[0]);
     const float pz = pos<ARITH>(az, a.voxel[2], a.origin[2]);
-    const uint32_t TW = M.TW;
+    const uint32_t pitch = tgt.x;
     if (ARITH == kFast) {
-        const float Cu = col_fast(M.cu, px, pz), Cv = col_fast(M.cv, px, pz), Cw = col_fast(M.cw, px, pz);
+        const uint4 fb = M.fast;
+        const float Cu = col_fast(cu, px, pz), Cv = col_fast(cv, px, pz), Cw = col_fast(cw, px, pz);
         const float hv = a.half_minus_off;
-        if (M.column) {
+        if (M.flags.z) {
             const float rw = __frcp_rn(Cw);
-            const float yu = __fmaf_rn(Cu, rw, 0.5f);
-            const bool in_u = (yu >= M.fu0) && (yu < M.fu1);
-            if (!__any_sync(0xffffffffu, in_u)) return;
-            const uint32_t K = __float_as_uint(__fadd_rz(yu, 8388608.0f)) - M.CT;
-            const float cvy = M.cv[1];
+            const uint32_t du = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x);
+            const bool in_u = du < fb.y;
+            if (!__any_sync(0xffffffffu, in_u)) return false;
+            const uint32_t K = du + tgt.y;
+            const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float yv = __fmaf_rn(__fmaf_rn(cvy, py[k], Cv), rw, hv);
-                const bool in = in_u && (yv >= M.fv0) && (yv < M.fv1);
-                f(k, in, __float_as_uint(__fadd_rz(yv, 8388608.0f)) * TW + K);
+                const uint32_t dv = fdist(__fmaf_rn(py[k], Qv, Rv), fb.z);
+                f(k, in_u && (dv < fb.w), dv * pitch + K);
             }
         } else {
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float nu = __fmaf_rn(M.cu[1], py[k], Cu);
-                const float nv = __fmaf_rn(M.cv[1], py[k], Cv);
-                const float nw = __fmaf_rn(M.cw[1], py[k], Cw);
-                const float rw = __frcp_rn(nw);
-                const float yu = __fmaf_rn(nu, rw, 0.5f);
-                const float yv = __fmaf_rn(nv, rw, hv);
-                const bool in = (yu >= M.fu0) && (yu < M.fu1) && (yv >= M.fv0) && (yv < M.fv1);
-                f(k, in, __float_as_uint(__fadd_rz(yv, 8388608.0f)) * TW +
-                             __float_as_uint(__fadd_rz(yu, 8388608.0f)) - M.CT);
+                const float rw = __frcp_rn(__fmaf_rn(cw.y, py[k], Cw));
+                const uint32_t du = fdist(__fmaf_rn(py[k], __fmul_rn(cu.y, rw), __fmaf_rn(Cu, rw, 0.5f)), fb.x);
+                const uint32_t dv = fdist(__fmaf_rn(py[k], __fmul_rn(cv.y, rw), __fmaf_rn(Cv, rw, hv)), fb.z);
+                f(k, (du < fb.y) && (dv < fb.w), dv * pitch + du + tgt.y);
             }
         }
     } else {
+        const int4 rc = M.rect;
         const float off = a.row_off_f;
-        if (M.column) {
+        if (M.flags.z) {
             // c.y == 0 in the u and w rows: c.y*py is a zero for every voxel of the column,
             // so n_u and n_w (up to the sign of a zero, which never changes a pixel) are
             // column invariants
-            const float nu = num_strict(M.cu, px, 0.0f, pz);
-            const float nw = num_strict(M.cw, px, 0.0f, pz);
-            const int iu = __float2int_rz(roundf(__fdiv_rn(nu, nw)));
-            const bool in_u = (iu >= M.u0) && (iu < M.u1);
-            if (!__any_sync(0xffffffffu, in_u)) return;
-            const uint32_t K = (uint32_t)iu - M.CS;
-            const float Pv = __fmul_rn(M.cv[0], px), Rv = __fmul_rn(M.cv[2], pz);
+            const float nu = num_strict(cu, px, 0.0f, pz);
+            const float nw = num_strict(cw, px, 0.0f, pz);
+            const uint32_t du = (uint32_t)(__float2int_rz(roundf(__fdiv_rn(nu, nw))) - rc.x);
+            const bool in_u = du < (uint32_t)rc.y;
+            if (!__any_sync(0xffffffffu, in_u)) return false;
+            const uint32_t K = du + tgt.y;
+            const float Pv = __fmul_rn(cv.x, px), Rv = __fmul_rn(cv.z, pz);
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float nv = __fadd_rn(__fadd_rn(__fadd_rn(Pv, __fmul_rn(M.cv[1], py[k])), Rv), M.cv[3]);
-                const int iv = __float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off)));
-                const bool in = in_u && (iv >= M.v0) && (iv < M.v1);
-                f(k, in, (uint32_t)iv * TW + K);
+                const float nv = __fadd_rn(__fadd_rn(__fadd_rn(Pv, __fmul_rn(cv.y, py[k])), Rv), cv.w);
+                const uint32_t dv = (uint32_t)(__float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off))) - rc.z);
+                f(k, in_u && (dv < (uint32_t)rc.w), dv * pitch + K);
             }
         } else {
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float nu = num_strict(M.cu, px, py[k], pz);
-                const float nv = num_strict(M.cv, px, py[k], pz);
-                const float nw = num_strict(M.cw, px, py[k], pz);
-                const int iu = __float2int_rz(roundf(__fdiv_rn(nu, nw)));
-                const int iv = __float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off)));
-                const bool in = (iu >= M.u0) && (iu < M.u1) && (iv >= M.v0) && (iv < M.v1);
-                f(k, in, (uint32_t)iv * TW + (uint32_t)iu - M.CS);
+                const float nu = num_strict(cu, px, py[k], pz);
+                const float nv = num_strict(cv, px, py[k], pz);
+                const float nw = num_strict(cw, px, py[k], pz);
+                const uint32_t du = (uint32_t)(__float2int_rz(roundf(__fdiv_rn(nu, nw))) - rc.x);
+                const uint32_t dv = (uint32_t)(__float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off))) - rc.z);
+                f(k, (du < (uint32_t)rc.y) && (dv < (uint32_t)rc.w), dv * pitch + du + tgt.y);
             }
         }
     }
+    return true;
 }
 
 // --------------------------------------------------------------------------------------
@@ -296,10 +292,10 @@ __global__ void __launch_bounds__(NT, 4)
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
             const ProjMeta &M = s_meta[g];
-            const int mode = M.mode;
-            if (mode == kSkip) continue;
+            const int4 fl = M.flags;
+            if (fl.x == kSkip) continue;
             uint32_t *tile = s_tile + g * TILE_CAP;
-            const bool orx = M.orient_x;
+            const bool orx = fl.y;
             // 4 columns per thread; lanes run across the ray so a warp hits distinct pixels
 #pragma unroll 1
             for (int j = 0; j < 4; ++j) {
@@ -307,7 +303,7 @@ __global__ void __launch_bounds__(NT, 4)
                 const int cz = orx ? lane : warp + 8 * j;
                 const uint32_t *vals = s_val + cz * VSTRIDE + cx;
                 const int ax = a.vmin[0] + x0 + cx, az = a.vmin[2] + z0 + cz;
-                if (mode == kTile) {
+                if (fl.x == kTile) {
                     walk_column<ARITH, BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
                         const uint32_t v = vals[k * BZ * VSTRIDE];
                         if (in & (v != 0u)) atomicAdd(&tile[idx], v);
@@ -325,11 +321,12 @@ __global__ void __launch_bounds__(NT, 4)
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
             const ProjMeta &M = s_meta[g];
-            if (M.mode != kTile) continue;
+            if (M.flags.x != kTile) continue;
             uint32_t *tile = s_tile + g * TILE_CAP;
-            const int tw = M.tw, th = M.v1 - M.v0;
+            const int4 rc = M.rect;
+            const int tw = rc.y, th = rc.w;
             for (int r = warp; r < th; r += NT / 32) {
-                uint32_t *dst = sum + M.img_base + (uint32_t)(M.v0 + r) * a.det_w + (uint32_t)M.u0;
+                uint32_t *dst = sum + M.tgt.z + (uint32_t)(rc.z + r) * a.det_w + (uint32_t)rc.x;
                 for (int c = lane; c < tw; c += 32) {
                     const uint32_t v = tile[r * tw + c];
                     if (v) {
@@ -378,11 +375,11 @@ __global__ void k_pad_items(float *vol, uint32_t *sum, const void *ratio, const 
         int iu, iv;
         bool in;
         if (ARITH == kFast) {
-            const float nu = __fmaf_rn(m[1], py, col_fast(m + 0, px, pz));
-            const float nv = __fmaf_rn(m[5], py, col_fast(m + 4, px, pz));
-            const float nw = __fmaf_rn(m[13], py, col_fast(m + 12, px, pz));
-            const float rw = __frcp_rn(nw);
-            const float yu = __fmaf_rn(nu, rw, 0.5f), yv = __fmaf_rn(nv, rw, a.half_minus_off);
+            const float4 c0 = make_float4(m[0], m[1], m[2], m[3]), c1 = make_float4(m[4], m[5], m[6], m[7]);
+            const float4 c3 = make_float4(m[12], m[13], m[14], m[15]);
+            const float rw = __frcp_rn(__fmaf_rn(c3.y, py, col_fast(c3, px, pz)));
+            const float yu = __fmaf_rn(py, __fmul_rn(c0.y, rw), __fmaf_rn(col_fast(c0, px, pz), rw, 0.5f));
+            const float yv = __fmaf_rn(py, __fmul_rn(c1.y, rw), __fmaf_rn(col_fast(c1, px, pz), rw, a.half_minus_off));
             in = yu >= (float)l && yu < (float)r && yv >= (float)bb && yv < (float)t;
             iu = in ? (int)floorf(yu) : 0;
             iv = in ? (int)floorf(yv) : 0;
@@ -437,17 +434,16 @@ __global__ void __launch_bounds__(NT, 3)
     const int x0 = bxi * BX, y0 = byi * BWD_BY, z0 = bzi * BWD_BZ;
     // thread = the voxel column (x0 + lane, z0 + warp), layers y0 .. y0 + BWD_BY
     const int ax = a.vmin[0] + x0 + lane, az = a.vmin[2] + z0 + warp;
-    constexpr int HB = BWD_BY / 2;  // gathers are issued in two batches of HB
 
     float py[BWD_BY], s[BWD_BY];
-    uint32_t n2[HB];  // in-bounds counts, two 16-bit halves per word (k even: low, odd: high)
+    uint32_t n2[BWD_BY / 2];  // in-bounds counts, two 16-bit halves per word (k even: low, odd: high)
 #pragma unroll
     for (int k = 0; k < BWD_BY; ++k) {
         py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
         s[k] = 0.0f;
     }
 #pragma unroll
-    for (int k = 0; k < HB; ++k) n2[k] = 0u;
+    for (int k = 0; k < BWD_BY / 2; ++k) n2[k] = 0u;
 
     for (int e0 = 0; e0 < (int)a.n_entries; e0 += G) {
         if (warp == 0)
@@ -456,33 +452,26 @@ __global__ void __launch_bounds__(NT, 3)
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
             const ProjMeta &M = s_meta[g];
-            if (M.mode == kSkip) continue;
-            // gathers index the whole image (compute_meta<.., GATHER = true>); the column's
-            // indices are computed first so all its loads are in flight together
-            uint32_t idx[BWD_BY];
-            uint32_t inmask = 0u;
-            walk_column<ARITH, BWD_BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t i) {
-                idx[k] = i;
-                inmask |= (in ? 1u : 0u) << k;
+            if (M.flags.x == kSkip) continue;
+            // the column's gathers are issued before any is consumed (all in flight together);
+            // an out-of-bounds pair contributes r = 0, and s + 0 == s exactly (s is never -0)
+            float r[BWD_BY];
+            const bool walked = walk_column<ARITH, BWD_BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
+                r[k] = 0.0f;
+                if (in) r[k] = load_ratio<DT>(ratio, idx);
+                if (!NANSKIP && in) n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
+                if (NANSKIP && !in) r[k] = __int_as_float(0x7fc00000);
             });
-            if (inmask == 0u) continue;
+            if (!walked) continue;  // warp-uniform
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                float r[HB];
-#pragma unroll
-                for (int q = 0; q < HB; ++q) {
-                    const int k = h * HB + q;
-                    r[q] = 0.0f;
-                    if (inmask & (1u << k)) r[q] = load_ratio<DT>(ratio, idx[k]);
-                }
-#pragma unroll
-                for (int q = 0; q < HB; ++q) {
-                    const int k = h * HB + q;
-                    const bool take = ((inmask >> k) & 1u) && (!NANSKIP || r[q] == r[q]);
-                    if (take) {
-                        s[k] = __fadd_rn(s[k], r[q]);
+            for (int k = 0; k < BWD_BY; ++k) {
+                if (NANSKIP) {
+                    if (r[k] == r[k]) {
+                        s[k] = __fadd_rn(s[k], r[k]);
                         n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
                     }
+                } else {
+                    s[k] = __fadd_rn(s[k], r[k]);
                 }
             }
         }

@@ -7,9 +7,11 @@
 //           n_r = ((c.x*px + c.y*py) + c.z*pz) + c.w for r in {u, v, w};
 //           u = n_u / n_w, v = n_v / n_w - line_offset; pixel = round half away
 //           from zero, converted with saturation (NaN -> 0).
-//   FAST    p = fma(idx, vx, o); n_r = fma(c.x, px, fma(c.y, py, c.w)) + c.z*pz;
-//           rw = 1/n_w (IEEE); yu = fma(n_u, rw, 0.5), yv = fma(n_v, rw, 0.5 - off);
-//           pixel = (floor(yu), floor(yv)).
+//   FAST    p = fma(idx, vx, o); C_r = fma(c.x, px, c.w) + c.z*pz for r in {u, v, w};
+//           rw = 1/fma(c_w.y, py, C_w) (IEEE); yu = fma(py, c_u.y*rw, fma(C_u, rw, 0.5)),
+//           yv = fma(py, c_v.y*rw, fma(C_v, rw, 0.5 - off)); pixel = (floor(yu), floor(yv)).
+//           For an untilted detector c_u.y = c_w.y = 0 exactly, so along a vertical voxel
+//           column u, w and 1/w are invariant and yv moves by one fma per voxel.
 //
 // Every operation is written with an explicit rounding intrinsic so that no
 // compiler contraction can change a result.  exp / log are this project's own
