@@ -180,6 +180,40 @@ int xpr_geometry(const xpr_geom_params *gp, int fp64, xpr_projdata *out, xpr_geo
  * from std::mt19937(seed) (reconstruction.hpp:268-272), 3 per sub-iteration. */
 int xpr_jitter(uint32_t seed, uint64_t n, float vx, float *out);
 
+/* method_2 chunk planner (GeometryChunk, geometry_chunk.hpp:92-197).  all: ProjData of
+ * every (angle, module).  chunks: 6 int64 per chunk {vOffset, vSize, iOffset, iSize,
+ * vPadTop, vPadBot}.  *n_chunks = -1 when one layer does not fit. */
+int xpr_plan_chunks(const xpr_geom_params *gp, const xpr_geom_out *go, const xpr_projdata *all, uint64_t avail_bytes,
+                    uint64_t max_alloc_bytes, float overlap_fct, int64_t *chunks, int max_chunks, int *n_chunks);
+/* method_1c per-layer angle culling (Geometry::getMvpPerLayer, geometry.hpp:141-171).
+ * per_module != 0 indexes ProjData by angle*modules + module (the reference indexes by
+ * angle, which is right for one module only). */
+int xpr_cull_layer(const xpr_geom_params *gp, const xpr_geom_out *go, const xpr_projdata *all, int64_t sit,
+                   int64_t layer, int per_module, uint16_t *mvp_idx, uint16_t *img_idx, int *n);
+
+/* ---------------------------------------------------------------- whole runs (host) */
+/* The XPRecon command line (main.cpp:69-136) as a call: json_or_path is a parameter
+ * file or inline JSON starting with '{'.  Runs the selected method (naive | method_1a |
+ * method_1b | method_1c | method_2) on the TIFF stack of recon.input, writes
+ * layer_%05d.tif to recon.output, then the simulation projections (p_%010d.tif) to
+ * recon.proj_output when set.  Returns 0, -2 (bad parameters) or -3 (reconstruction
+ * error), the reference's exit codes. */
+int xpr_run(const char *json_or_path);
+/* The default parameters as JSON (XPRecon -template).  Returns the length; writes at
+ * most cap bytes (NUL-terminated) when buf is non-NULL. */
+int64_t xpr_template_json(char *buf, uint64_t cap);
+/* The parameters a run would use (defaults, aliases, initializeParameters applied), as JSON. */
+int xpr_params_normalize(const char *json_or_path, char *buf, uint64_t cap, int64_t *len);
+/* A whole reconstruction of in-memory projections (count images of height x width floats,
+ * acquisition order) with the parameters of `json` (recon.input / output unused, no files
+ * written).  vol_out receives vwidth * vheight * vwidth floats; layers a method does not
+ * reconstruct (method_2 outside its chunks) are NaN.  *seconds: time of the iterations. */
+int xpr_reconstruct_host(const char *json, const float *images, int64_t count, uint32_t width, uint32_t height,
+                         float *vol_out, uint64_t vol_cap, double *seconds);
+/* Single-channel float32 TIFF I/O (the reference uses TinyTIFF, data_loader.hpp:209-237). */
+int xpr_tiff_write(const char *path, const float *data, uint32_t width, uint32_t height);
+int xpr_tiff_read(const char *path, float *data, uint64_t cap, uint32_t *width, uint32_t *height);
+
 #ifdef __cplusplus
 }
 #endif

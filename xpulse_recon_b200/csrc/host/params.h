@@ -1,0 +1,90 @@
+// params.h -- the XPRecon parameter schema.
+//
+// Keys and defaults follow src/reconstruction/dataset/parameters/global_parameters.hpp:8-55
+// and specialized_parameters.hpp:22-39; loading follows dataset/parameters.hpp:34-84
+// (a path, or inline JSON when the argument starts with '{'; rx is converted from
+// pixels to mm after loading).  Extensions of this backend (all optional):
+//   recon.seed           origin-jitter seed (absent: std::random_device, as the reference)
+//   recon.arith          "fast" | "strict"  projector arithmetic contract
+//   recon.storage        "fp32" | "bf16" | "fp16"  detector image / ratio storage
+//   recon.geometry       "fp32" | "fp64"  precision of the matrix construction (fp32: the
+//                        reference's single-precision glm construction, the default)
+//   recon.compat_pad     reproduce the reference's NDRange padding work-items (naive)
+//   recon.mem_cap        device-memory cap, bytes or "64G" / "512M"
+//   recon.device         CUDA device ordinal
+//   recon.slab           layers per streamed y-slab in method_1a/1b/1c (0: as many as fit)
+//   recon.images_preproc alias of recon.normalize (the README's name for it)
+//   detector.modules[]   per-module {offset_x, offset_y, offset_z, roll, pitch, yaw}
+//                        (the reference's commented-out global_parameters.hpp:38-44, 51)
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "json.h"
+
+namespace xpr {
+
+enum class Method { naive, method_1a, method_1b, method_1c, method_2, hartmann, ipr };
+
+struct ModuleParams {
+    float offset_x = 0.0f, offset_y = 0.0f, offset_z = 0.0f;
+    float roll = 0.0f, pitch = 0.0f, yaw = 0.0f;
+};
+
+struct Params {
+    // recon (global_parameters.hpp:8-21)
+    std::string input = "./";
+    std::string output = "./recon/";
+    std::string proj_output = "";
+    Method method = Method::method_1b;
+    int64_t it = 1, sit = 10;
+    bool mlog = true;
+    float weight = 1.0f, weight_factor = 0.9f;
+    bool normalize = false;
+    bool simulation = false;
+    // geometry (:23-36)
+    float so = 100.0f, sd = 1000.0f, angle = 360.0f;
+    float heli_offset = 0.0f, heli_step = 1.0f;
+    std::vector<float> angle_list;
+    // detector (:46-54)
+    float px = 0.1f, rx = 0.0f, sx = 0.0f, sy = 0.0f;  // rx in pixels as read; rx_mm() after loading
+    int64_t module_number = 1;
+    bool module_angle_offset_set = false;
+    float module_angle_offset = 0.0f;
+    float module_center_offset_z = 0.0f;
+    std::vector<ModuleParams> modules;
+    // method2 (specialized_parameters.hpp:34-39)
+    float overlap_fct = 1.0f;
+    // hartmann / ipr (kept for the schema and -template; the methods are not implemented here)
+    std::string hm_devx = "./", hm_devy = "./";
+    float hm_iterations = 0.0f, hm_iterations_fct = 1.0f;
+    int64_t hm_iterations_step = 1;
+    std::string hm_method = "gs";
+    float ipr_iterations = 0.0f, ipr_iterations_fct = 1.0f;
+    int64_t ipr_iterations_step = 1;
+    float ipr_energy_kev = 1.0f;
+    // extensions
+    bool seed_set = false;
+    uint32_t seed = 0;
+    std::string arith = "fast";
+    std::string storage = "fp32";
+    std::string geometry = "fp32";
+    bool compat_pad = false;
+    uint64_t mem_cap = 0;
+    int device = 0;
+    int64_t slab = 0;
+};
+
+const char *method_name(Method m);
+
+// Parse a parameter file path or an inline JSON string (starting with '{'), apply
+// initializeParameters (parameters.hpp:34-48).  Throws std::runtime_error.
+Params load_params(const std::string &file_or_content);
+Params params_from_json(const json::Value &root);
+// The default parameter set serialised as JSON (XPRecon -template, main.cpp:75-79).
+std::string params_to_json(const Params &p);
+uint64_t parse_bytes(const std::string &s);
+
+}  // namespace xpr
