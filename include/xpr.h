@@ -149,6 +149,23 @@ int xpr_subiteration(xpr_ctx *ctx, float *vol, uint32_t *sum, const void *images
                      int ratio_dtype, const xpr_projdata *pd, uint32_t n_pd, const xpr_launch *L, float weight,
                      int first, double *residual, void *stream);
 
+/* One sub-iteration as xpr_subiteration, for callers that cannot allocate device
+ * memory while they run (a host application that owns the device budget and passes
+ * only its inputs and outputs; a frame loop that must not stall on, or fail in, an
+ * allocation).  No counterpart in the reference.  The detector scratch (fixed-point
+ * sums, overwritten in place by the FP32 ratio) lives in a fixed device array of
+ * xpr_subiteration_static_capacity() 32-bit words, held by every GPU that loads the
+ * library until the process exits; larger sub-iterations (n_angles * det_w * rows
+ * words) are rejected with XPR_ERR_CAP.  The call neither allocates nor frees.  It
+ * starts from FIXED_ONE sums when first != 0 (forward skipped) and from zero sums
+ * otherwise, so no state carries over between calls; the ratio is FP32.  The first
+ * call on a device looks up the array's device address; make that first call before
+ * any stream capture.  All calls share the one array: calls that overlap on the GPU
+ * (other streams, other threads) race on it. */
+int xpr_subiteration_static(xpr_ctx *ctx, float *vol, const void *images, int image_dtype, const xpr_projdata *pd,
+                            uint32_t n_pd, const xpr_launch *L, float weight, int first, void *stream);
+uint64_t xpr_subiteration_static_capacity(void);
+
 /* ---------------------------------------------------------------- geometry (host) */
 /* Geometry parameters (global_parameters.hpp:23-54, parameters.hpp:34-48). */
 typedef struct xpr_geom_params {

@@ -56,6 +56,35 @@ inline bool valid_dtype(int d) { return d == XPR_F32 || d == XPR_BF16 || d == XP
 
 }  // namespace
 
+namespace xpr {
+
+const DeviceInfo *context_device(xpr_ctx *ctx)
+{
+    if (!ctx) {
+        fail(XPR_ERR_INVALID, "context is NULL");
+        return nullptr;
+    }
+    const cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) {
+        cuda_fail(e, "cudaSetDevice");
+        return nullptr;
+    }
+    return &ctx->dev;
+}
+
+int set_last_error(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+}  // namespace xpr
+
 extern "C" {
 
 const char *xpr_last_error(void) { return g_last_error.c_str(); }

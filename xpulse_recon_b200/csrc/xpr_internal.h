@@ -53,4 +53,10 @@ cudaError_t launch_convert(const float *src, void *dst, int dtype, uint64_t n, c
 // One-time per-device kernel attributes (dynamic shared memory opt-in).
 cudaError_t prepare_device_kernels();
 
+// For entry points defined outside xpr_capi.cu: make ctx's device current and return
+// its description (nullptr and a message on failure), and record an error message
+// for xpr_last_error(); returns `code`.
+const DeviceInfo *context_device(xpr_ctx *ctx);
+int set_last_error(int code, const char *fmt, ...);
+
 }  // namespace xpr
