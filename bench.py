@@ -49,6 +49,10 @@ CONFIGS = {
 
 FLOPS_PER_PAIR = 44          # algorithmic FP32 operations per (voxel, projection) pair, forward + backward
 NOMINAL_FP32_LANES = 148 * 128
+# DRAM bytes (read + write) per voxel per launch, from one ncu capture of each kernel on the
+# c2 geometry's central 256-layer slab (FAST contract, FP32 storage: 717.3 MB and 1210.2 MB
+# for 150,994,944 voxels); scaled to a launch by its voxel count for the same geometry
+MEASURED_TRAFFIC_PER_VOXEL = {"forward": 717.3e6 / 150994944, "backward": 1210.2e6 / 150994944}
 
 
 def parse_args():
@@ -491,6 +495,9 @@ def run_ours(args, cfg, rank, world, local):
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     achieved = alg_bytes / (dom_ms / 1000.0) / 1e9
+    traffic = None
+    if args.config in ("c2", "c2slab") and args.storage == "fp32":
+        traffic = MEASURED_TRAFFIC_PER_VOXEL[dom] * prob.nvox
     sm_mhz = (clk or {}).get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = NOMINAL_FP32_LANES * 2 * float(sm_mhz) * 1e6 / 1e12
     step_ms = total_ms / K
@@ -507,8 +514,10 @@ def run_ours(args, cfg, rank, world, local):
         "gpu_launches": 3 * K,
         "kernels_ms": {"forward": f_ms, "error": statistics.mean(err), "backward": b_ms},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "note": "issue/atomic-bound (not a dense contraction, not HBM-bound): see compute"},
+                     "frac": achieved / hbm, "traffic": traffic,
+                     "algorithmic_bytes": alg_bytes,
+                     "note": "issue/atomic-bound (not a dense contraction, not HBM-bound): see compute; "
+                             "traffic scaled from an ncu capture of the 256-layer slab by voxel count"},
         "compute": {"flops_per_pair": FLOPS_PER_PAIR, "achieved_tflops": FLOPS_PER_PAIR * pairs_step / (step_ms / 1000) / 1e12,
                     "peak_fp32_tflops": fp32_peak, "frac": FLOPS_PER_PAIR * pairs_step / (step_ms / 1000) / 1e12 / fp32_peak,
                     "peak_source": "nominal: 148 SM x 128 FP32 lanes x 2 x median SM clock"},
