@@ -344,8 +344,10 @@ def cpu_reference_step_factory(cfg, seconds_target):
             O.backward(vol, sums.view(np.float32), pd, L)
         return time.perf_counter() - t, n * Pc
 
-    dt, pairs = run(1)
-    layers = int(max(1, min(Hv, round(seconds_target / max(dt, 1e-3)))))
+    # calibrate on a few layers (one layer is dominated by fixed costs), then size the sample
+    probe = min(8, Hv)
+    dt, pairs = run(probe)
+    layers = int(max(1, min(Hv, round(probe * seconds_target / max(dt, 1e-3)))))
     info = {"kind": kind, "cores": os.cpu_count(), "layers": layers, "W": W, "Pc": Pc}
     return (lambda: run(layers)), info
 

@@ -103,6 +103,13 @@ def lib():
             getattr(L, fn).argtypes = [C.POINTER(GeomParams), C.POINTER(ReconParams), f32p, f32p]
         L.orc_recon_chunks.restype = C.c_int
         L.orc_recon_chunks.argtypes = [C.POINTER(GeomParams), C.POINTER(ReconParams), f32p, i64p, C.c_int, f32p]
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        L.orc_geometry_f64.argtypes = [C.POINTER(GeomParams), f64p, f64p, C.POINTER(GeomOut)]
+        L.orc64_forward.argtypes = [f64p, f64p, f64p, f64p, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                                    C.POINTER(C.c_double), C.c_double, C.c_int64, C.c_int64]
+        L.orc64_preprocess.argtypes = [f32p, f64p, C.c_uint64, C.c_int]
+        L.orc64_recon_naive.restype = C.c_int
+        L.orc64_recon_naive.argtypes = [C.POINTER(GeomParams), C.POINTER(ReconParams), f64p, f64p]
         _oracle = L
     return _oracle
 
@@ -244,3 +251,38 @@ def ref_backward(vol, ratio, pd, det_w, det_h, origin, n_angles, modules, vmin, 
 def ref_error(images, sums, det_w, det_h, weight):
     R = ref_lib()
     R.refk_error(images, sums, _c_arr(C.c_uint32, [det_w, det_h, det_w, 1]), sums.size, weight, ndrange(sums.size))
+
+
+# ----------------------------------------------------------------------------- FP64 oracle
+def geometry_f64(g: GeomParams):
+    """(mvp float64[P*M, 16], vp float64[P*M, 4], GeomOut): the geometry in double."""
+    n = g.projections * g.module_number
+    mvp = np.zeros((n, 16), np.float64)
+    vp = np.zeros((n, 4), np.float64)
+    go = GeomOut()
+    lib().orc_geometry_f64(C.byref(g), mvp, vp, C.byref(go))
+    return mvp, vp, go
+
+
+def forward_f64(vol, mvp, vp, modules, W, Hv, origin, voxel, det_w, rows):
+    """Double-precision forward of a W x Hv x W volume against len(mvp) (angle, module)
+    entries; returns the detector sums, float64[len(mvp) // modules, rows, det_w]."""
+    n_img = mvp.shape[0] // modules
+    out = np.zeros(n_img * rows * det_w, np.float64)
+    o = (C.c_double * 3)(*origin)
+    lib().orc64_forward(np.ascontiguousarray(vol, np.float64).ravel(), out, np.ascontiguousarray(mvp),
+                        np.ascontiguousarray(vp), mvp.shape[0], modules, W, Hv, o, voxel, det_w, rows)
+    return out.reshape(n_img, rows, det_w)
+
+
+def recon_naive_f64(gp: GeomParams, rp: ReconParams, raw: np.ndarray, mlog: bool = True) -> np.ndarray:
+    """The naive reconstruction in double from raw (un-preprocessed) float32 images."""
+    raw = np.ascontiguousarray(raw, np.float32).ravel()
+    imgs = np.zeros(raw.size, np.float64)
+    lib().orc64_preprocess(raw, imgs, raw.size, int(mlog))
+    go = GeomOut()
+    tmp = np.zeros((gp.projections * gp.module_number, 20), np.float32)
+    lib().orc_geometry(C.byref(gp), 1, tmp, C.byref(go))
+    vol = np.zeros(int(go.vwidth) * int(go.vheight) * int(go.vwidth), np.float64)
+    assert lib().orc64_recon_naive(C.byref(gp), C.byref(rp), imgs, vol) == 0
+    return vol

@@ -516,6 +516,70 @@ static m4d gen_proj_d(v3d pe, v3d pa, v3d pb, v3d pc, double vpl, double vpr, do
     return m4d_mul(m4d_mul(m4d_mul(m4d_rows(T), m4d_rows(Mt)), m4d_rows(P)), m4d_rows(S));
 }
 
+/* The geometry of orc_geometry in double precision end to end (matrices kept in double):
+ * column-major mvp (16 per entry) and viewport {l, r, b, t} (4 per entry). */
+static void geometry_f64(const orc_geom_params *gp, int64_t P, int64_t M, uint64_t width, uint64_t height,
+                         double *mvp_out, double *vp_out)
+{
+    const double so = gp->so, sd = gp->sd, px = gp->px;
+    v3d dsource_pos = {0.0, 0.0, 0.0};
+    v3d dsource_at = {0.0, 0.0, sd};
+    v3d daxis = v3d_add(dsource_at, (v3d){-(double)gp->sx + (double)gp->rx_px * px, -(double)gp->sy, 0.0});
+    v3d dcenter = v3d_mul(v3d_norm(daxis), so);
+    dsource_pos = v3d_sub(dsource_pos, dcenter);
+    dsource_at = v3d_sub(dsource_at, dcenter);
+    v3d zero = {0.0, 0.0, 0.0};
+    for (int64_t i = 0; i < P; ++i) {
+        double heli = ((double)gp->heli_offset / (double)P) * (double)i - (double)gp->heli_offset * 0.5;
+        double angle_deg = gp->angle_list ? (double)gp->angle_list[i] : (double)i * ((double)gp->angle / (double)P);
+        v3d rsp = v3d_add(rotate_xyz_d(dsource_pos, zero, 0.0, angle_deg, 0.0), (v3d){0.0, heli, 0.0});
+        v3d rsa = v3d_add(rotate_xyz_d(dsource_at, zero, 0.0, angle_deg, 0.0), (v3d){0.0, heli, 0.0});
+        for (int64_t mod = 0; mod < M; ++mod) {
+            v3d vv = {0.0, 1.0, 0.0};
+            v3d dir = v3d_sub(rsa, rsp);
+            v3d u = v3d_norm(v3d_cross(vv, dir));
+            v3d nrm = v3d_norm(dir);
+            v3d detector = v3d_sub(v3d_sub(rsa, v3d_mul(u, gp->sx)), v3d_mul(vv, gp->sy));
+            if (gp->mod_offset) {
+                const float *o = gp->mod_offset + 3 * mod;
+                detector = v3d_add(detector, v3d_add(v3d_add(v3d_mul(u, o[0] * px), v3d_mul(vv, o[1] * px)),
+                                                     v3d_mul(nrm, o[2] * px)));
+            }
+            v3d ul = v3d_sub(v3d_sub(detector, v3d_mul(u, 0.5 * (double)width * px)),
+                             v3d_mul(vv, 0.5 * (double)height * px));
+            v3d ur = v3d_add(ul, v3d_mul(u, (double)width * px));
+            v3d bl = v3d_add(ul, v3d_mul(vv, (double)height * px));
+            if (gp->mod_rpy) {
+                const float *a = gp->mod_rpy + 3 * mod;
+                v3d *cs[3] = {&ul, &ur, &bl};
+                for (int c = 0; c < 3; ++c) {
+                    v3d w = v3d_sub(*cs[c], detector);
+                    w = rotate_axis_d(w, a[2] * ORC_DEG2RAD, u);
+                    w = rotate_axis_d(w, a[1] * ORC_DEG2RAD, vv);
+                    w = rotate_axis_d(w, a[0] * ORC_DEG2RAD, nrm);
+                    *cs[c] = v3d_add(w, detector);
+                }
+            }
+            v3d center = detector;
+            v3d mc = v3d_add(center, v3d_mul(v3d_norm(v3d_sub(rsp, rsa)), sd - (double)gp->module_center_offset_z));
+            double dist = sqrt(v3d_dot(v3d_sub(center, mc), v3d_sub(center, mc)));
+            double mang = gp->module_angle_offset_set
+                              ? (double)gp->module_angle_offset
+                              : (2.0 * atan2((double)width * 0.5 * px, dist)) * 57.295779513082320877;
+            double mcur = mang * ((double)mod - floor((double)M / 2.0));
+            v3d pa = rotate_xyz_d(ul, mc, 0.0, mcur, 0.0);
+            v3d pb = rotate_xyz_d(ur, mc, 0.0, mcur, 0.0);
+            v3d pc = rotate_xyz_d(bl, mc, 0.0, mcur, 0.0);
+            double vpl = (double)(width * (uint64_t)mod), vpr = (double)(width * (uint64_t)(mod + 1));
+            m4d mvp = gen_proj_d(rsp, pa, pb, pc, vpl, vpr, 0.0, (double)gp->dheight, sd);
+            double *om = mvp_out + (i * M + mod) * 16, *ov = vp_out + (i * M + mod) * 4;
+            for (int c = 0; c < 4; ++c)
+                for (int r = 0; r < 4; ++r) om[c * 4 + r] = mvp.c[c][r];
+            ov[0] = vpl; ov[1] = vpr; ov[2] = 0.0; ov[3] = (double)gp->dheight;
+        }
+    }
+}
+
 int orc_geometry(const orc_geom_params *gp, int fp64, orc_projdata *out, orc_geom_out *go)
 {
     const int64_t P = gp->projections, M = gp->module_number;
@@ -594,63 +658,15 @@ int orc_geometry(const orc_geom_params *gp, int fp64, orc_projdata *out, orc_geo
             }
         }
     } else {
-        const double so = gp->so, sd = gp->sd, px = gp->px;
-        v3d dsource_pos = {0.0, 0.0, 0.0};
-        v3d dsource_at = {0.0, 0.0, sd};
-        v3d daxis = v3d_add(dsource_at, (v3d){-(double)gp->sx + (double)gp->rx_px * px, -(double)gp->sy, 0.0});
-        v3d dcenter = v3d_mul(v3d_norm(daxis), so);
-        dsource_pos = v3d_sub(dsource_pos, dcenter);
-        dsource_at = v3d_sub(dsource_at, dcenter);
-        v3d zero = {0.0, 0.0, 0.0};
-        for (int64_t i = 0; i < P; ++i) {
-            double heli = ((double)gp->heli_offset / (double)P) * (double)i - (double)gp->heli_offset * 0.5;
-            double angle_deg = gp->angle_list ? (double)gp->angle_list[i] : (double)i * ((double)gp->angle / (double)P);
-            v3d rsp = v3d_add(rotate_xyz_d(dsource_pos, zero, 0.0, angle_deg, 0.0), (v3d){0.0, heli, 0.0});
-            v3d rsa = v3d_add(rotate_xyz_d(dsource_at, zero, 0.0, angle_deg, 0.0), (v3d){0.0, heli, 0.0});
-            for (int64_t mod = 0; mod < M; ++mod) {
-                v3d vv = {0.0, 1.0, 0.0};
-                v3d dir = v3d_sub(rsa, rsp);
-                v3d u = v3d_norm(v3d_cross(vv, dir));
-                v3d nrm = v3d_norm(dir);
-                v3d detector = v3d_sub(v3d_sub(rsa, v3d_mul(u, gp->sx)), v3d_mul(vv, gp->sy));
-                if (gp->mod_offset) {
-                    const float *o = gp->mod_offset + 3 * mod;
-                    detector = v3d_add(detector, v3d_add(v3d_add(v3d_mul(u, o[0] * px), v3d_mul(vv, o[1] * px)),
-                                                         v3d_mul(nrm, o[2] * px)));
-                }
-                v3d ul = v3d_sub(v3d_sub(detector, v3d_mul(u, 0.5 * (double)width * px)),
-                                 v3d_mul(vv, 0.5 * (double)height * px));
-                v3d ur = v3d_add(ul, v3d_mul(u, (double)width * px));
-                v3d bl = v3d_add(ul, v3d_mul(vv, (double)height * px));
-                if (gp->mod_rpy) {
-                    const float *a = gp->mod_rpy + 3 * mod;
-                    v3d *cs[3] = {&ul, &ur, &bl};
-                    for (int c = 0; c < 3; ++c) {
-                        v3d w = v3d_sub(*cs[c], detector);
-                        w = rotate_axis_d(w, a[2] * ORC_DEG2RAD, u);
-                        w = rotate_axis_d(w, a[1] * ORC_DEG2RAD, vv);
-                        w = rotate_axis_d(w, a[0] * ORC_DEG2RAD, nrm);
-                        *cs[c] = v3d_add(w, detector);
-                    }
-                }
-                v3d center = detector;
-                v3d mc = v3d_add(center, v3d_mul(v3d_norm(v3d_sub(rsp, rsa)), sd - (double)gp->module_center_offset_z));
-                double dist = sqrt(v3d_dot(v3d_sub(center, mc), v3d_sub(center, mc)));
-                double mang = gp->module_angle_offset_set
-                                  ? (double)gp->module_angle_offset
-                                  : (2.0 * atan2((double)width * 0.5 * px, dist)) * 57.295779513082320877;
-                double mcur = mang * ((double)mod - floor((double)M / 2.0));
-                v3d pa = rotate_xyz_d(ul, mc, 0.0, mcur, 0.0);
-                v3d pb = rotate_xyz_d(ur, mc, 0.0, mcur, 0.0);
-                v3d pc = rotate_xyz_d(bl, mc, 0.0, mcur, 0.0);
-                double vpl = (double)(width * (uint64_t)mod), vpr = (double)(width * (uint64_t)(mod + 1));
-                m4d mvp = gen_proj_d(rsp, pa, pb, pc, vpl, vpr, 0.0, (double)gp->dheight, sd);
-                orc_projdata *o = &out[i * M + mod];
-                for (int c = 0; c < 4; ++c)
-                    for (int r = 0; r < 4; ++r) o->mvp[c * 4 + r] = (float)mvp.c[c][r];
-                o->vp[0] = (float)vpl; o->vp[1] = (float)vpr; o->vp[2] = 0.0f; o->vp[3] = (float)gp->dheight;
-            }
+        double *dm = (double *)malloc(sizeof(double) * (size_t)(P * M * 16));
+        double *dv = (double *)malloc(sizeof(double) * (size_t)(P * M * 4));
+        geometry_f64(gp, P, M, width, height, dm, dv);
+        for (int64_t k = 0; k < P * M; ++k) {
+            for (int j = 0; j < 16; ++j) out[k].mvp[j] = (float)dm[k * 16 + j];
+            for (int j = 0; j < 4; ++j) out[k].vp[j] = (float)dv[k * 4 + j];
         }
+        free(dm);
+        free(dv);
     }
     return 0;
 }
@@ -1001,5 +1017,145 @@ int orc_recon_chunks(const orc_geom_params *gp, const orc_recon_params *rp, cons
     }
     free(pd);
     free(all);
+    return 0;
+}
+
+/* ======================================================================== */
+/* FP64 oracle: the algorithm in double precision with no fixed point       */
+/* ======================================================================== */
+/* The precision reference for reduced-precision storage.  It keeps everything
+ * that defines the algorithm -- the geometry of geometry.hpp (built and kept in
+ * double), the same mt19937 jitter draws (uniform_real_distribution<float>, then
+ * widened), the nearest-pixel rule with the viewport bounds, the clamps of the
+ * error step (eps = 2^-22, KernelError.cl:8-24) and of the -log preprocessing
+ * (data_loader.hpp:84-86), 0/0 -> NaN for voxels no projection reaches -- and drops
+ * what only exists for single precision: the 22-bit fixed-point sums (double sums
+ * instead) and the float roundings. */
+int orc_geometry_f64(const orc_geom_params *gp, double *mvp, double *vp, orc_geom_out *go)
+{
+    const int64_t P = gp->projections, M = gp->module_number;
+    orc_projdata *tmp = (orc_projdata *)malloc(sizeof(orc_projdata) * (size_t)(P * M));
+    orc_geometry(gp, 1, tmp, go);
+    free(tmp);
+    geometry_f64(gp, P, M, (uint64_t)gp->dwidth / (uint64_t)M, (uint64_t)gp->dheight, mvp, vp);
+    return 0;
+}
+
+static inline int pair_f64(const double *m, const double *vp, double px, double py, double pz, double rows,
+                           int64_t *iu, int64_t *iv)
+{
+    const double nu = m[0] * px + m[1] * py + m[2] * pz + m[3];
+    const double nv = m[4] * px + m[5] * py + m[6] * pz + m[7];
+    const double nw = m[12] * px + m[13] * py + m[14] * pz + m[15];
+    const double yu = nu / nw + 0.5, yv = nv / nw + 0.5;
+    const int in = (yu >= vp[0]) && (yu < vp[1]) && (yv >= vp[2]) && (yv < vp[3]) && (yv < rows);
+    if (in) {
+        *iu = (int64_t)floor(yu);
+        *iv = (int64_t)floor(yv);
+    }
+    return in;
+}
+
+void orc64_forward(const double *vol, double *sum, const double *mvp, const double *vp, int64_t n_entries,
+                   int64_t modules, int64_t W, int64_t Hv, const double origin[3], double voxel, int64_t det_w,
+                   int64_t rows)
+{
+    const int64_t n = W * Hv * W, stride = det_w * rows;
+#pragma omp parallel for schedule(static, 4096)
+    for (int64_t id = 0; id < n; ++id) {
+        const int64_t y = id / (W * W), z = (id / W) % W, x = id % W;
+        const double px = (double)x * voxel + origin[0], py = (double)y * voxel + origin[1],
+                     pz = (double)z * voxel + origin[2];
+        const double value = vol[id];
+        if (value == 0.0) continue;
+        for (int64_t e = 0; e < n_entries; ++e) {
+            int64_t iu, iv;
+            if (!pair_f64(mvp + 16 * e, vp + 4 * e, px, py, pz, (double)rows, &iu, &iv)) continue;
+            double *dst = &sum[(e / modules) * stride + iv * det_w + iu];
+#pragma omp atomic
+            *dst += value;
+        }
+    }
+}
+
+void orc64_backward(double *vol, const double *ratio, const double *mvp, const double *vp, int64_t n_entries,
+                    int64_t modules, int64_t W, int64_t Hv, const double origin[3], double voxel, int64_t det_w,
+                    int64_t rows)
+{
+    const int64_t n = W * Hv * W, stride = det_w * rows;
+#pragma omp parallel for schedule(static, 4096)
+    for (int64_t id = 0; id < n; ++id) {
+        const int64_t y = id / (W * W), z = (id / W) % W, x = id % W;
+        const double px = (double)x * voxel + origin[0], py = (double)y * voxel + origin[1],
+                     pz = (double)z * voxel + origin[2];
+        double s = 0.0;
+        int64_t cnt = 0;
+        for (int64_t e = 0; e < n_entries; ++e) {
+            int64_t iu, iv;
+            if (!pair_f64(mvp + 16 * e, vp + 4 * e, px, py, pz, (double)rows, &iu, &iv)) continue;
+            s += ratio[(e / modules) * stride + iv * det_w + iu];
+            ++cnt;
+        }
+        vol[id] *= exp(s / (double)cnt);
+    }
+}
+
+void orc64_preprocess(const float *raw, double *out, uint64_t n, int mlog)
+{
+    const double eps = 1.0 / 4194304.0;
+#pragma omp parallel for schedule(static, 65536)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        double x = (double)raw[i];
+        if (mlog) x = -log(fmax(fmin(x, 1.0 - eps), eps));
+        out[i] = x;
+    }
+}
+
+int orc64_recon_naive(const orc_geom_params *gp, const orc_recon_params *rp, const double *images, double *vol)
+{
+    orc_geom_out go;
+    const int64_t P = gp->projections, M = gp->module_number, S = rp->sit;
+    orc_geom_params g = *gp;
+    g.sit = S;
+    double *mvp = (double *)malloc(sizeof(double) * (size_t)(P * M * 16));
+    double *vp = (double *)malloc(sizeof(double) * (size_t)(P * M * 4));
+    orc_geometry_f64(&g, mvp, vp, &go);
+    const int64_t Pc = go.concurrent, W = go.vwidth, Hv = go.vheight, Wd = gp->dwidth, Hd = gp->dheight;
+    if (Pc <= 0) { free(mvp); free(vp); return -1; }
+    const double eps = 1.0 / 4194304.0;
+    const int64_t n_sum = Pc * Wd * Hd, nvox = W * Hv * W;
+    double *sum = (double *)malloc(sizeof(double) * (size_t)n_sum);
+    double *smvp = (double *)malloc(sizeof(double) * (size_t)(Pc * M * 16));
+    double *svp = (double *)malloc(sizeof(double) * (size_t)(Pc * M * 4));
+    for (int64_t i = 0; i < nvox; ++i) vol[i] = 1.0;
+    orc_mt19937 gen;
+    orc_mt_seed(&gen, rp->seed);
+    double weight = rp->weight;
+    for (int64_t mit = 0; mit < rp->it; ++mit) {
+        for (int64_t sit = 0; sit < S; ++sit) {
+            double origin[3];
+            for (int i = 0; i < 3; ++i) origin[i] = (double)go.orig[i] + (double)orc_uniform_float(&gen, 0.0f, go.vx);
+            for (int64_t k = 0; k < Pc; ++k)
+                for (int64_t mod = 0; mod < M; ++mod) {
+                    memcpy(smvp + (k * M + mod) * 16, mvp + ((sit + k * S) * M + mod) * 16, sizeof(double) * 16);
+                    memcpy(svp + (k * M + mod) * 4, vp + ((sit + k * S) * M + mod) * 4, sizeof(double) * 4);
+                }
+            if (sit > 0 || mit > 0) {
+                memset(sum, 0, sizeof(double) * (size_t)n_sum);
+                orc64_forward(vol, sum, smvp, svp, Pc * M, M, W, Hv, origin, (double)go.vx, Wd, Hd);
+            } else {
+                for (int64_t i = 0; i < n_sum; ++i) sum[i] = 1.0;
+            }
+#pragma omp parallel for schedule(static, 65536)
+            for (int64_t i = 0; i < n_sum; ++i) {
+                const int64_t k = i / (Wd * Hd), r = i - k * Wd * Hd;
+                const double ref = images[(sit + k * S) * Wd * Hd + r];
+                sum[i] = log(fmax(ref / fmax(sum[i], eps), eps)) * weight;
+            }
+            orc64_backward(vol, sum, smvp, svp, Pc * M, M, W, Hv, origin, (double)go.vx, Wd, Hd);
+        }
+        weight *= rp->weight_factor;
+    }
+    free(sum); free(smvp); free(svp); free(mvp); free(vp);
     return 0;
 }

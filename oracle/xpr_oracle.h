@@ -174,6 +174,20 @@ int orc_recon_1c(const orc_geom_params *gp, const orc_recon_params *rp,
 int orc_recon_chunks(const orc_geom_params *gp, const orc_recon_params *rp,
                      const float *images, const int64_t *chunks, int n_chunks, float *vol);
 
+/* ---- FP64 oracle: the same algorithm in double, no fixed point ----------
+ * The precision reference for reduced-precision storage (xpr_oracle.c). */
+int orc_geometry_f64(const orc_geom_params *gp, double *mvp, double *vp, orc_geom_out *go);
+void orc64_forward(const double *vol, double *sum, const double *mvp, const double *vp, int64_t n_entries,
+                   int64_t modules, int64_t W, int64_t Hv, const double origin[3], double voxel, int64_t det_w,
+                   int64_t rows);
+void orc64_backward(double *vol, const double *ratio, const double *mvp, const double *vp, int64_t n_entries,
+                    int64_t modules, int64_t W, int64_t Hv, const double origin[3], double voxel, int64_t det_w,
+                    int64_t rows);
+void orc64_preprocess(const float *raw, double *out, uint64_t n, int mlog);
+/* naive method in double: images = P preprocessed images in file order,
+ * vol = W*H*W doubles */
+int orc64_recon_naive(const orc_geom_params *gp, const orc_recon_params *rp, const double *images, double *vol);
+
 #ifdef __cplusplus
 }
 #endif

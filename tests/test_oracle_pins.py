@@ -243,3 +243,59 @@ def test_exports_match_header(xlib):
     assert len(names) >= 20
     missing = [n for n in names if not hasattr(xlib, n)]
     assert not missing, missing
+
+
+# ----------------------------------------------------------------------------- FP64 oracle
+def test_fp64_geometry_rounds_to_the_fp64_projdata():
+    gp = O.geom_params(dwidth=40, dheight=24, projections=12, sit=3, module_number=2, rx=1.5, sx=-2.0, sy=3.0,
+                       mod_rpy=np.array([1.0, -0.5, 0.8, 0.0, 0.3, -1.2], np.float32))
+    mvp, vp, go = O.geometry_f64(gp)
+    pd, go2 = O.geometry(gp, fp64=True)
+    np.testing.assert_array_equal(mvp.astype(np.float32), pd[:, :16])
+    np.testing.assert_array_equal(vp.astype(np.float32), pd[:, 16:])
+    assert go.vx == go2.vx and go.vwidth == go2.vwidth
+
+
+def test_fp64_oracle_agrees_with_fp32_oracle_on_consistent_data():
+    """The FP64 reconstruction (no fixed point) against the single-precision oracle with
+    the same double-built matrices, on Poisson-noisy projections (1e5 photons) of a ball
+    phantom.  (On noise-free data the empty background's measured values sit at the
+    2^-22 clamp, the resolution of the 22-bit fixed-point sums, and the two diverge
+    there by construction.)"""
+    gp = O.geom_params(dwidth=48, dheight=40, projections=40, sit=4, rx=1.0, sx=-0.5, sy=0.8)
+    mvp, vp, go = O.geometry_f64(gp)
+    W, Hv = int(go.vwidth), int(go.vheight)
+    yy, zz, xx = np.meshgrid(np.arange(Hv), np.arange(W), np.arange(W), indexing="ij")
+    ph = np.where((xx - W / 2) ** 2 + (zz - W / 2) ** 2 + 1.5 * (yy - Hv / 2) ** 2 < (0.3 * W) ** 2, 0.01, 0.0)
+    p = O.forward_f64(ph, mvp, vp, 1, W, Hv, [float(go.orig[i]) + 0.5 * go.vx for i in range(3)], go.vx, 48, 40)
+    assert 0.2 < p.max() < 1.0
+    counts = np.random.default_rng(3).poisson(1e5 * np.exp(-p))
+    raw = (np.maximum(counts, 1) / 1e5).astype(np.float32)
+    rp = O.ReconParams(2, 4, 1.0, 0.9, 77, O.FAST, 0)
+    v64 = O.recon_naive_f64(gp, rp, raw)
+    # single precision, same double-built matrices, same jitter draws
+    pd_all, _ = O.geometry(gp, fp64=True)
+    imgs = raw.ravel().copy()
+    O.lib().orc_preprocess(imgs, imgs.size, 0, 0.0, 0.0, 1)
+    imgs = imgs.reshape(40, 40, 48)
+    vol = np.ones(W * Hv * W, np.float32)
+    sums = np.full(10 * 48 * 40, 1 << 22, np.uint32)
+    g = O.MT()
+    O.lib().orc_mt_seed(O.C.byref(g), 77)
+    w = np.float32(1.0)
+    for mit in range(2):
+        for s in range(4):
+            origin = [float(np.float32(go.orig[i]) + np.float32(O.lib().orc_uniform_float(O.C.byref(g), 0.0, go.vx)))
+                      for i in range(3)]
+            pd = np.ascontiguousarray(O.subset_projdata(pd_all, 40, 4, 1, s, 10), np.float32)
+            L, keep = O.make_launch((0, 0, 0), (W, Hv, W), origin, [go.vx] * 3, 48, 40, 0, 10, 1, arith=O.FAST)
+            if mit or s:
+                O.forward(vol, sums, pd, L)
+            O.error(np.ascontiguousarray(imgs[[s + 4 * k for k in range(10)]]).ravel(), sums, float(w))
+            O.backward(vol, sums.view(np.float32), pd, L)
+            sums[:] = 0
+        w = np.float32(w * np.float32(0.9))
+    np.testing.assert_array_equal(np.isnan(vol), np.isnan(v64))
+    m = np.isfinite(v64)
+    rel = np.sqrt(np.mean((vol[m] - v64[m]) ** 2)) / np.sqrt(np.mean(v64[m] ** 2))
+    assert rel < 1e-3, rel
