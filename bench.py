@@ -45,6 +45,12 @@ CONFIGS = {
     "c1": dict(desc="192^3 recon grid (128^3 phantom: 10 ellipsoids), 180 projections of 192x192, sit=10 -> 18",
                dwidth=192, dheight=192, projections=180, sit=10, px=0.1, so=100.0, sd=1000.0, rx=0.0, sx=0.0,
                sy=0.0, phantom=128, ellipsoids=10, background=0.0, i0=1e5, seed=1),
+    # many small reconstructions as one batched, graph-captured, autotuned run (BF16 storage)
+    "c4": dict(desc="64 independent 384^3 recon grids (256^3 ellipsoid phantoms, so U[80,120], sd U[800,1200]), "
+                    "360 projections of 384x384 on 3 modules of 128 px (roll/pitch/yaw U[-2,2] deg), sit=10 -> 36, "
+                    "it=2, BF16 image/ratio storage, one batched persistent launch per phase in a CUDA graph",
+               batch=64, dwidth=384, dheight=384, projections=360, sit=10, it=2, modules=3, px=0.1, rpy=2.0,
+               phantom=256, ellipsoids=12, background=0.0, i0=1e5, seed=4, plain_sample=4),
 }
 
 FLOPS_PER_PAIR = 44          # algorithmic FP32 operations per (voxel, projection) pair, forward + backward
@@ -538,12 +544,161 @@ def run_ours(args, cfg, rank, world, local):
     return 0
 
 
+# ----------------------------------------------------------------------------- batched (c4)
+def run_batched(args, cfg, rank, world, local):
+    """Many small reconstructions in one batched run (xpr_batch: persistent launches over
+    all problems, the whole it x sit run captured into a CUDA graph, autotuned schedule),
+    BF16 image / ratio storage; beside it the plain FP32 path (one problem at a time,
+    one xpr_subiteration per sub-iteration) on a sample of the same problems."""
+    import torch
+    from xpulse_recon_b200 import _lib
+    from xpulse_recon_b200.batch import Batch, Problem as BProblem, torch_dtype
+    from xpulse_recon_b200.projector import Context, geometry
+    torch.cuda.set_device(local)
+    L = _lib.lib()
+    ctx = Context(local)
+    rng = np.random.default_rng(cfg["seed"] + 1000 * rank)
+    storage = {"fp32": _lib.F32, "bf16": _lib.BF16, "fp16": _lib.F16}[args.storage if args.storage != "fp32"
+                                                                       else "bf16"]
+    S, it, M, P = cfg["sit"], cfg["it"], cfg["modules"], cfg["projections"]
+    Wd, Hd = cfg["dwidth"], cfg["dheight"]
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    probs, plain_imgs = [], []
+    for i in range(cfg["batch"]):
+        so, sd = float(rng.uniform(80, 120)), float(rng.uniform(800, 1200))
+        rpy = rng.uniform(-cfg["rpy"], cfg["rpy"], 3 * M).astype(np.float32)
+        pd_all, g = geometry(so=so, sd=sd, px=cfg["px"], dwidth=Wd, dheight=Hd, projections=P, sit=S,
+                             module_number=M, mod_rpy=rpy)
+        W, Hv, Pc = int(g["vwidth"]), int(g["vheight"]), int(g["concurrent"])
+        phantom = make_phantom(cfg, g["vx"], W, Hv, "cuda", int(rng.integers(1 << 30)))
+        sums = torch.zeros(P * Wd * Hd, dtype=torch.int32, device="cuda")
+        d = _lib.Launch()
+        d.vmax[:] = [W, Hv, W]
+        d.origin[:] = list(g["orig"])
+        d.voxel[:] = [g["vx"]] * 3
+        d.det_w, d.rows, d.n_angles, d.modules, d.arith = Wd, Hd, P, M, _lib.FAST
+        dpd = torch.from_numpy(pd_all).cuda()
+        _lib.check(L.xpr_forward(ctx.handle, phantom.data_ptr(), sums.data_ptr(), dpd.data_ptr(), P * M,
+                                 C.byref(d), sp), "forward")
+        p = sums.to(torch.int64).bitwise_and(0xFFFFFFFF).to(torch.float32) / float(1 << 22)
+        gen = torch.Generator(device="cuda").manual_seed(int(rng.integers(1 << 30)))
+        raw = (torch.poisson(cfg["i0"] * torch.exp(-p), generator=gen) / cfg["i0"]).view(P, Hd, Wd)
+        order = torch.tensor([s + k * S for s in range(S) for k in range(Pc)], device="cuda")
+        raw_sub = raw[order].reshape(-1).contiguous()
+        del sums, p, raw, phantom
+        pd = torch.from_numpy(np.ascontiguousarray(pd_all.reshape(P, M, 20)[order.cpu().numpy()].reshape(-1, 20)))
+        imgs = torch.empty(raw_sub.numel(), dtype=torch_dtype(storage), device="cuda")
+        _lib.check(L.xpr_preprocess_apply(ctx.handle, raw_sub.data_ptr(), imgs.data_ptr(), storage, raw_sub.numel(),
+                                          0, None, 1, sp), "preprocess")
+        if i < cfg["plain_sample"]:
+            f32 = torch.empty(raw_sub.numel(), dtype=torch.float32, device="cuda")
+            _lib.check(L.xpr_preprocess_apply(ctx.handle, raw_sub.data_ptr(), f32.data_ptr(), _lib.F32,
+                                              raw_sub.numel(), 0, None, 1, sp), "preprocess")
+            plain_imgs.append(f32)
+        del raw_sub
+        probs.append(BProblem(vol=torch.ones(W * Hv * W, dtype=torch.float32, device="cuda"), images=imgs,
+                              projdata=pd.cuda(), det_w=Wd, det_h=Hd, per_subset=Pc, modules=M, sit=S, it=it,
+                              vwidth=W, vheight=Hv, voxel=float(g["vx"]), orig=tuple(g["orig"]),
+                              seed=int(rng.integers(1 << 31)), weight=1.0, weight_factor=0.9))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b = Batch(ctx, probs, arith=_lib.FAST, storage=storage, use_graph=True, autotune=True)
+    tune_s = time.perf_counter() - t0
+    steps = b.steps
+    pairs_step = sum(p.vwidth * p.vheight * p.vwidth * p.per_subset for p in probs)
+    runs_w = max(1, -(-args.warmup // steps))
+    runs_t = max(1, -(-args.steps // steps))
+    for _ in range(runs_w):
+        b.run()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(runs_t):
+        b.run()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    n_steps = runs_t * steps
+    value = pairs_step * n_steps / (ms / 1000.0) / 1e9
+    # the plain FP32 path on a sample of the same problems, one at a time
+    plain_ms, plain_pairs = 0.0, 0
+    for i, f32 in enumerate(plain_imgs):
+        p = probs[i]
+        q = BProblem(vol=torch.ones_like(p.vol), images=f32, projdata=p.projdata, det_w=Wd, det_h=Hd,
+                     per_subset=p.per_subset, modules=M, sit=S, it=it, vwidth=p.vwidth, vheight=p.vheight,
+                     voxel=p.voxel, orig=p.orig, seed=p.seed)
+        q.run_alone(ctx, _lib.FAST, _lib.F32)  # warm
+        torch.cuda.synchronize()
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        q.run_alone(ctx, _lib.FAST, _lib.F32)
+        z.record()
+        torch.cuda.synchronize()
+        plain_ms += a.elapsed_time(z)
+        plain_pairs += p.vwidth * p.vheight * p.vwidth * p.per_subset * p.it * p.sit
+    plain = plain_pairs / (plain_ms / 1000.0) / 1e9 if plain_ms else None
+    sch = b.schedule()
+
+    # the same sample: alone in the batch's storage, and batched in FP32 / the batch's storage
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        z.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(z)
+
+    sample = []
+    for i, f32 in enumerate(plain_imgs):
+        p = probs[i]
+        sample.append((p, BProblem(vol=torch.ones_like(p.vol), images=f32, projdata=p.projdata, det_w=Wd, det_h=Hd,
+                                   per_subset=p.per_subset, modules=M, sit=S, it=it, vwidth=p.vwidth,
+                                   vheight=p.vheight, voxel=p.voxel, orig=p.orig, seed=p.seed)))
+    breakdown = {}
+    if sample:
+        alone_st = sum(timed(lambda p=p: p.run_alone(ctx, _lib.FAST, storage)) for p, _ in sample)
+        bq = Batch(ctx, [q for _, q in sample], arith=_lib.FAST, storage=_lib.F32, use_graph=True, autotune=True)
+        batch_f32 = timed(bq.run)
+        bq.close()
+        bs = Batch(ctx, [p for p, _ in sample], arith=_lib.FAST, storage=storage, use_graph=True, autotune=True)
+        batch_st = timed(bs.run)
+        bs.close()
+        g = lambda ms: plain_pairs / (ms / 1000.0) / 1e9  # noqa: E731
+        breakdown = {"alone_fp32": plain, "alone_storage": g(alone_st), "batched_fp32": g(batch_f32),
+                     "batched_storage": g(batch_st)}
+    line = {"metric": "GUPS per sub-iteration (voxel x projection pairs / s)", "value": value, "unit": "GUPS",
+            "n_gpus": world, "steps": n_steps, "warmup": runs_w * steps, "ms_per_step": ms / n_steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"bf16": "bf16 storage, f32 compute", "fp16": "fp16 storage, f32 compute",
+                      "fp32": "f32"}[{_lib.BF16: "bf16", _lib.F16: "fp16", _lib.F32: "fp32"}[storage]],
+            "data": "synthetic", "config": {"workload": "c4: " + cfg["desc"], "problems": len(probs),
+                                            "steps_per_run": steps, "l2": "inputs larger than L2 (%.1f GB)"
+                                            % (sum(p.vol.numel() * 4 for p in probs) / 1e9)},
+            "module_pairs_gups": value * M, "schedule": sch, "autotune_s": tune_s,
+            "plain_fp32": {"value": plain, "unit": "GUPS", "sample": "%d of the %d problems, each alone, FP32, "
+                           "one xpr_subiteration per sub-iteration" % (len(plain_imgs), len(probs))},
+            "speedup_vs_plain_fp32": (value / plain) if plain else None, "sample_gups": breakdown,
+            "gpu_launches": 3 * n_steps, "clocks": clk}
+    if rank == 0:
+        emit(line)
+    b.close()
+    return 0
+
+
 def main():
     args = parse_args()
     cfg = CONFIGS[args.config]
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, cfg, rank, world)
+    if "batch" in cfg:
+        return run_batched(args, cfg, rank, world, local)
     return run_ours(args, cfg, rank, world, local)
 
 

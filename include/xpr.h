@@ -166,6 +166,59 @@ int xpr_subiteration_static(xpr_ctx *ctx, float *vol, const void *images, int im
                             uint32_t n_pd, const xpr_launch *L, float weight, int first, void *stream);
 uint64_t xpr_subiteration_static_capacity(void);
 
+/* ---------------------------------------------------------------- batched reconstructions */
+/* Many independent naive reconstructions (reconstruction_n.hpp:27-88 each) advanced in
+ * lock-step.  A sub-iteration step of all problems is three persistent launches (forward,
+ * error, backward) whose CTAs claim work units from one list spanning every problem;
+ * a whole run can be captured once into a CUDA graph and replayed.  No counterpart in
+ * the reference, which runs one reconstruction per process.  Each problem's volume is
+ * bit-identical to the same reconstruction run alone through xpr_subiteration (same
+ * seed, contract and storage), whatever the batch, schedule or tuning. */
+typedef struct xpr_batch_problem {
+    float *vol;                   /* device, vwidth * vheight * vwidth floats (x fastest, then z, then y) */
+    const void *images;           /* device, sit * per_subset preprocessed images of det_w * det_h in the batch's
+                                     storage type, subset-major: subset s holds acquisitions s, s + sit, ... */
+    const xpr_projdata *projdata; /* device, sit * per_subset * modules entries in the same order */
+    uint32_t det_w, det_h;
+    uint32_t per_subset;          /* projections per sub-iteration: floor(projections / sit) */
+    uint32_t modules;
+    uint32_t sit, it;
+    uint32_t vwidth, vheight;     /* the reconstruction grid (geometry.hpp:55-60) */
+    float voxel;                  /* vx */
+    float orig[3];                /* grid origin before the jitter */
+    uint32_t seed;                /* std::mt19937 seed of the origin jitter (3 draws per sub-iteration) */
+    float weight, weight_factor;
+    double *residual;             /* optional device array of it * sit doubles: sum of ratio^2 per sub-iteration */
+} xpr_batch_problem;
+
+typedef struct xpr_batch_opts {
+    int32_t arith;                /* xpr_arith */
+    int32_t storage;              /* xpr_dtype of the images and of the ratio scratch */
+    int32_t init_volume;          /* each run first sets every volume to 1.0 (reconstruction_n.hpp:59) */
+    int32_t use_graph;            /* capture the whole run into one CUDA graph at the first run, replay after */
+    int32_t autotune;             /* time the schedule candidates once (per batch shape, cached) */
+    int32_t fwd_splits;           /* 0: automatic or tuned; else projection runs per forward brick */
+    int32_t bwd_column;           /* 0: automatic or tuned; else 8 or 16 layers per backward voxel column */
+    int32_t ctas_per_sm;          /* 0: the occupancy limit */
+} xpr_batch_opts;
+
+typedef struct xpr_batch xpr_batch;
+/* Validates the problems, allocates their scratch (fixed-point sums and ratios) through
+ * ctx and uploads every step's work lists.  With opts->autotune it runs the candidate
+ * schedules on the problems' data (volumes are left as they were). */
+int xpr_batch_create(xpr_ctx *ctx, const xpr_batch_problem *problems, uint32_t n, const xpr_batch_opts *opts,
+                     void *stream, xpr_batch **out);
+/* All it * sit sub-iterations of every problem (the longest problem sets the step count). */
+int xpr_batch_run(xpr_batch *b, void *stream);
+/* One step: sub-iteration `step` of every problem that has one (step < xpr_batch_steps). */
+int xpr_batch_step(xpr_batch *b, uint32_t step, void *stream);
+uint32_t xpr_batch_steps(const xpr_batch *b);
+/* The schedule in use: projection runs per forward brick, backward column length,
+ * persistent CTAs per SM, and the tuned step time in ms (0 when not tuned). */
+int xpr_batch_schedule(const xpr_batch *b, int32_t *fwd_splits, int32_t *bwd_column, int32_t *ctas_per_sm,
+                       double *tuned_ms);
+int xpr_batch_destroy(xpr_batch *b);
+
 /* ---------------------------------------------------------------- geometry (host) */
 /* Geometry parameters (global_parameters.hpp:23-54, parameters.hpp:34-48). */
 typedef struct xpr_geom_params {

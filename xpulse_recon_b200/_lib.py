@@ -52,6 +52,22 @@ class GeomOut(C.Structure):
                 ("orig", C.c_float * 3), ("concurrent", C.c_int64)]
 
 
+class BatchProblem(C.Structure):
+    _fields_ = [
+        ("vol", C.c_void_p), ("images", C.c_void_p), ("projdata", C.c_void_p),
+        ("det_w", C.c_uint32), ("det_h", C.c_uint32), ("per_subset", C.c_uint32), ("modules", C.c_uint32),
+        ("sit", C.c_uint32), ("it", C.c_uint32), ("vwidth", C.c_uint32), ("vheight", C.c_uint32),
+        ("voxel", C.c_float), ("orig", C.c_float * 3), ("seed", C.c_uint32),
+        ("weight", C.c_float), ("weight_factor", C.c_float), ("residual", C.c_void_p),
+    ]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("arith", C.c_int32), ("storage", C.c_int32), ("init_volume", C.c_int32),
+                ("use_graph", C.c_int32), ("autotune", C.c_int32), ("fwd_splits", C.c_int32),
+                ("bwd_column", C.c_int32), ("ctas_per_sm", C.c_int32)]
+
+
 _lib = None
 vp = C.c_void_p
 u64 = C.c_uint64
@@ -95,6 +111,14 @@ def lib():
                                       C.c_float, i32, vp, vp])
     _sig(L, "xpr_geometry", i32, [C.POINTER(GeomParams), i32, vp, C.POINTER(GeomOut)])
     _sig(L, "xpr_jitter", i32, [C.c_uint32, u64, C.c_float, vp])
+    _sig(L, "xpr_batch_create", i32, [vp, C.POINTER(BatchProblem), C.c_uint32, C.POINTER(BatchOpts), vp,
+                                      C.POINTER(vp)])
+    _sig(L, "xpr_batch_run", i32, [vp, vp])
+    _sig(L, "xpr_batch_step", i32, [vp, C.c_uint32, vp])
+    _sig(L, "xpr_batch_steps", C.c_uint32, [vp])
+    _sig(L, "xpr_batch_schedule", i32, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_double)])
+    _sig(L, "xpr_batch_destroy", i32, [vp])
     _lib = L
     return L
 

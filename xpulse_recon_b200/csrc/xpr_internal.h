@@ -59,4 +59,55 @@ cudaError_t prepare_device_kernels();
 const DeviceInfo *context_device(xpr_ctx *ctx);
 int set_last_error(int code, const char *fmt, ...);
 
+// ---- batched launches: many independent problems in one persistent launch ----------
+// Device descriptors, one per problem; work units are numbered across the problems
+// (unit_begin = prefix sum of the problems' unit counts), claimed by persistent CTAs
+// from a self-resetting ticket (two words, zero before the first launch).
+struct BatchFwdItem {
+    LaunchArgs a;
+    const float *vol;
+    uint32_t *sum;
+    const xpr_projdata *pd;
+    int32_t bricks_x, bricks_z;
+    uint32_t splits;          // projection runs per brick (a.per_split entries each)
+    uint32_t unit_begin;
+};
+struct BatchBwdItem {
+    LaunchArgs a;
+    float *vol;
+    const void *ratio;
+    const xpr_projdata *pd;
+    int32_t bricks_x, bricks_z;
+    uint32_t unit_begin;
+    uint32_t reserved;
+};
+struct BatchErrItem {
+    const void *images;
+    uint32_t *sum;            // zeroed after it is read
+    void *ratio;
+    double *residual;         // optional: += sum of r^2 (FP64)
+    uint64_t n;
+    float weight;
+    int32_t first;            // 1: the first sub-iteration, sums taken as FIXED_ONE (no forward ran)
+};
+struct BatchFillItem {
+    uint32_t *dst;
+    uint64_t n;
+    uint32_t value;
+    uint32_t reserved;
+};
+
+// forward brick / backward brick extents (work-unit geometry for the host planner)
+int forward_brick(int axis);               // 0: x, 1: y, 2: z
+int backward_brick(int axis, int cb);
+int batched_ctas_per_sm(int kind, int arith, int dtype, int cb);  // kind 0: forward, 1: backward
+cudaError_t launch_forward_batched(const BatchFwdItem *items, int n_items, uint32_t total_units, uint32_t *ticket,
+                                   int arith, unsigned ctas, cudaStream_t s);
+cudaError_t launch_backward_batched(const BatchBwdItem *items, int n_items, uint32_t total_units, uint32_t *ticket,
+                                    int arith, int dtype, int cb, unsigned ctas, cudaStream_t s);
+cudaError_t launch_error_batched(const BatchErrItem *items, int n_items, int image_dtype, int ratio_dtype,
+                                 uint64_t max_n, const DeviceInfo &dev, cudaStream_t s);
+cudaError_t launch_fill_batched(const BatchFillItem *items, int n_items, uint64_t max_n, const DeviceInfo &dev,
+                                cudaStream_t s);
+
 }  // namespace xpr

@@ -248,18 +248,20 @@ __device__ __forceinline__ bool walk_column(const ProjMeta &M, const LaunchArgs 
 // --------------------------------------------------------------------------------------
 constexpr size_t kFwdSmem = (size_t)(BY * BZ * VSTRIDE + G * TILE_CAP) * sizeof(uint32_t);
 
+// One forward work unit: brick `brick` (x fastest, then z, then y) against the
+// projection run `split` (entries [split * per_split, (split + 1) * per_split)).
+// Called by every thread of the CTA; returns with the CTA converged.
 template <int ARITH, bool LIST>
-__global__ void __launch_bounds__(NT, 4)
-    k_forward_tiled(const float *__restrict__ vol, uint32_t *__restrict__ sum, const xpr_projdata *__restrict__ pd,
-                    const LaunchArgs a, int bricks_x, int bricks_z)
+__device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint32_t *__restrict__ sum,
+                                             const xpr_projdata *__restrict__ pd, const LaunchArgs &a,
+                                             uint32_t brick, uint32_t split, int bricks_x, int bricks_z,
+                                             uint32_t *smem, ProjMeta *s_meta)
 {
-    extern __shared__ uint32_t smem[];
     uint32_t *s_val = smem;                        // [BY][BZ][VSTRIDE] fixed-point values
     uint32_t *s_tile = smem + BY * BZ * VSTRIDE;   // [G][TILE_CAP]
-    __shared__ ProjMeta s_meta[G];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int b = blockIdx.x;
+    int b = (int)brick;
     const int bxi = b % bricks_x;
     b /= bricks_x;
     const int bzi = b % bricks_z;
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(NT, 4)
 #pragma unroll
     for (int k = 0; k < BY; ++k) py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
 
-    const int e_begin = blockIdx.y * (int)a.per_split;
+    const int e_begin = (int)split * (int)a.per_split;
     const int e_end = min((int)a.n_entries, e_begin + (int)a.per_split);
 
     for (int e0 = e_begin; e0 < e_end; e0 += G) {
@@ -338,6 +340,16 @@ __global__ void __launch_bounds__(NT, 4)
         }
         __syncthreads();
     }
+}
+
+template <int ARITH, bool LIST>
+__global__ void __launch_bounds__(NT, 4)
+    k_forward_tiled(const float *__restrict__ vol, uint32_t *__restrict__ sum, const xpr_projdata *__restrict__ pd,
+                    const LaunchArgs a, int bricks_x, int bricks_z)
+{
+    extern __shared__ uint32_t smem[];
+    __shared__ ProjMeta s_meta[G];
+    forward_unit<ARITH, LIST>(vol, sum, pd, a, blockIdx.x, blockIdx.y, bricks_x, bricks_z, smem, s_meta);
 }
 
 // Work-items of the reference NDRange padding (kernel.hpp:73-81, H5): one thread each,
@@ -419,35 +431,37 @@ __device__ __forceinline__ float load_ratio(const void *ratio, uint32_t i)
     return __half2float(__ldg((const __half *)ratio + i));
 }
 
-template <int ARITH, bool LIST, bool NANSKIP, int DT>
-__global__ void __launch_bounds__(NT, 3)
-    k_backward_tiled(float *__restrict__ vol, const void *__restrict__ ratio, const xpr_projdata *__restrict__ pd,
-                     const LaunchArgs a, int bricks_x, int bricks_z)
+// One backward work unit: the brick of 32 x CB x 8 voxels `brick` (x fastest, then z,
+// then y); every thread owns one voxel column of CB layers.  CB (16 or 8) trades
+// registers for fewer projection-metadata passes per voxel.
+template <int ARITH, bool LIST, bool NANSKIP, int DT, int CB>
+__device__ __forceinline__ void backward_unit(float *__restrict__ vol, const void *__restrict__ ratio,
+                                              const xpr_projdata *__restrict__ pd, const LaunchArgs &a,
+                                              uint32_t brick, int bricks_x, int bricks_z, ProjMeta *s_meta)
 {
-    __shared__ ProjMeta s_meta[G];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int b = blockIdx.x;
+    int b = (int)brick;
     const int bxi = b % bricks_x;
     b /= bricks_x;
     const int bzi = b % bricks_z;
     const int byi = b / bricks_z;
-    const int x0 = bxi * BX, y0 = byi * BWD_BY, z0 = bzi * BWD_BZ;
-    // thread = the voxel column (x0 + lane, z0 + warp), layers y0 .. y0 + BWD_BY
+    const int x0 = bxi * BX, y0 = byi * CB, z0 = bzi * BWD_BZ;
+    // thread = the voxel column (x0 + lane, z0 + warp), layers y0 .. y0 + CB
     const int ax = a.vmin[0] + x0 + lane, az = a.vmin[2] + z0 + warp;
 
-    float py[BWD_BY], s[BWD_BY];
-    uint32_t n2[BWD_BY / 2];  // in-bounds counts, two 16-bit halves per word (k even: low, odd: high)
+    float py[CB], s[CB];
+    uint32_t n2[CB / 2];  // in-bounds counts, two 16-bit halves per word (k even: low, odd: high)
 #pragma unroll
-    for (int k = 0; k < BWD_BY; ++k) {
+    for (int k = 0; k < CB; ++k) {
         py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
         s[k] = 0.0f;
     }
 #pragma unroll
-    for (int k = 0; k < BWD_BY / 2; ++k) n2[k] = 0u;
+    for (int k = 0; k < CB / 2; ++k) n2[k] = 0u;
 
     for (int e0 = 0; e0 < (int)a.n_entries; e0 += G) {
         if (warp == 0)
-            compute_meta<LIST, true>(s_meta, pd, a, e0, (int)a.n_entries, x0, y0, z0, BX, BWD_BY, BWD_BZ, lane);
+            compute_meta<LIST, true>(s_meta, pd, a, e0, (int)a.n_entries, x0, y0, z0, BX, CB, BWD_BZ, lane);
         __syncthreads();
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
@@ -455,8 +469,8 @@ __global__ void __launch_bounds__(NT, 3)
             if (M.flags.x == kSkip) continue;
             // the column's gathers are issued before any is consumed (all in flight together);
             // an out-of-bounds pair contributes r = 0, and s + 0 == s exactly (s is never -0)
-            float r[BWD_BY];
-            const bool walked = walk_column<ARITH, BWD_BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
+            float r[CB];
+            const bool walked = walk_column<ARITH, CB>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
                 r[k] = 0.0f;
                 if (in) r[k] = load_ratio<DT>(ratio, idx);
                 if (!NANSKIP && in) n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
@@ -464,7 +478,7 @@ __global__ void __launch_bounds__(NT, 3)
             });
             if (!walked) continue;  // warp-uniform
 #pragma unroll
-            for (int k = 0; k < BWD_BY; ++k) {
+            for (int k = 0; k < CB; ++k) {
                 if (NANSKIP) {
                     if (r[k] == r[k]) {
                         s[k] = __fadd_rn(s[k], r[k]);
@@ -479,9 +493,9 @@ __global__ void __launch_bounds__(NT, 3)
     }
     const int sx = a.size[0], sy = a.size[1], sz = a.size[2];
     const int x = x0 + lane, z = z0 + warp;
-    if (x >= sx || z >= sz) return;
+    if (x >= sx || z >= sz) return;  // after the last barrier of the unit
 #pragma unroll
-    for (int k = 0; k < BWD_BY; ++k) {
+    for (int k = 0; k < CB; ++k) {
         const int y = y0 + k;
         if (y < sy) {
             const uint32_t cnt = (k & 1) ? (n2[k >> 1] >> 16) : (n2[k >> 1] & 0xffffu);
@@ -489,6 +503,16 @@ __global__ void __launch_bounds__(NT, 3)
             *p = __fmul_rn(*p, p_expf(__fdiv_rn(s[k], __uint2float_rn(cnt))));
         }
     }
+}
+
+
+template <int ARITH, bool LIST, bool NANSKIP, int DT, int CB>
+__global__ void __launch_bounds__(NT, 3)
+    k_backward_tiled(float *__restrict__ vol, const void *__restrict__ ratio, const xpr_projdata *__restrict__ pd,
+                     const LaunchArgs a, int bricks_x, int bricks_z)
+{
+    __shared__ ProjMeta s_meta[G];
+    backward_unit<ARITH, LIST, NANSKIP, DT, CB>(vol, ratio, pd, a, blockIdx.x, bricks_x, bricks_z, s_meta);
 }
 
 // --------------------------------------------------------------------------------------
@@ -617,6 +641,124 @@ __global__ void k_convert(const float *__restrict__ x, void *out, uint64_t n)
 }
 
 // ======================================================================================
+// batched (persistent) kernels: many independent problems per launch
+// ======================================================================================
+// A CTA claims work units from ticket[0] until they run out; the last CTA to leave
+// (ticket[1] counts departures) puts both words back to zero for the next launch, so
+// a batch's launches need no reset between them and capture into a graph as is.
+__device__ __forceinline__ int find_item(const uint32_t *begins, size_t stride, int n_items, uint32_t unit)
+{
+    int lo = 0, hi = n_items - 1;  // last item with begin <= unit
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg((const uint32_t *)((const char *)begins + (size_t)mid * stride)) <= unit) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void ticket_depart(uint32_t *ticket)
+{
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ticket[1], 1u) == gridDim.x - 1) {
+            atomicExch(&ticket[0], 0u);
+            atomicExch(&ticket[1], 0u);
+        }
+    }
+}
+
+template <int ARITH>
+__global__ void __launch_bounds__(NT, 4)
+    k_forward_batched(const BatchFwdItem *__restrict__ items, int n_items, uint32_t total_units, uint32_t *ticket)
+{
+    extern __shared__ uint32_t smem[];
+    __shared__ ProjMeta s_meta[G];
+    __shared__ LaunchArgs s_a;
+    __shared__ uint32_t s_unit;
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t u = atomicAdd(&ticket[0], 1u);
+            int it = 0;
+            if (u < total_units) {
+                it = find_item(&items[0].unit_begin, sizeof(BatchFwdItem), n_items, u);
+                s_a = items[it].a;
+            }
+            s_unit = u;
+            s_item = it;
+        }
+        __syncthreads();
+        const uint32_t u = s_unit;
+        if (u >= total_units) break;
+        const BatchFwdItem &I = items[s_item];
+        const uint32_t local = u - I.unit_begin, splits = I.splits;
+        forward_unit<ARITH, false>(I.vol, I.sum, I.pd, s_a, local / splits, local % splits, I.bricks_x, I.bricks_z,
+                                   smem, s_meta);
+        __syncthreads();
+    }
+    ticket_depart(ticket);
+}
+
+template <int ARITH, int DT, int CB>
+__global__ void __launch_bounds__(NT, 3)
+    k_backward_batched(const BatchBwdItem *__restrict__ items, int n_items, uint32_t total_units, uint32_t *ticket)
+{
+    __shared__ ProjMeta s_meta[G];
+    __shared__ LaunchArgs s_a;
+    __shared__ uint32_t s_unit;
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t u = atomicAdd(&ticket[0], 1u);
+            int it = 0;
+            if (u < total_units) {
+                it = find_item(&items[0].unit_begin, sizeof(BatchBwdItem), n_items, u);
+                s_a = items[it].a;
+            }
+            s_unit = u;
+            s_item = it;
+        }
+        __syncthreads();
+        const uint32_t u = s_unit;
+        if (u >= total_units) break;
+        const BatchBwdItem &I = items[s_item];
+        backward_unit<ARITH, false, false, DT, CB>(I.vol, I.ratio, I.pd, s_a, u - I.unit_begin, I.bricks_x,
+                                                   I.bricks_z, s_meta);
+        __syncthreads();
+    }
+    ticket_depart(ticket);
+}
+
+// grid (x: chunks of an item, y: item)
+template <int IDT, int RDT>
+__global__ void k_error_batched(const BatchErrItem *__restrict__ items)
+{
+    const BatchErrItem I = items[blockIdx.y];
+    double acc = 0.0;
+    const bool resid = I.residual != nullptr;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < I.n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float ref = load_any<IDT>(I.images, i);
+        const float got = I.first ? 1.0f : fixed_to_float(I.sum[i]);
+        const float r = __fmul_rn(p_logf(fmaxf(__fdiv_rn(ref, fmaxf(got, kEps)), kEps)), I.weight);
+        store_any<RDT>(I.ratio, i, r);
+        I.sum[i] = 0u;
+        if (resid) acc += (double)r * (double)r;
+    }
+    if (resid) {
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(I.residual, acc);
+    }
+}
+
+__global__ void k_fill_batched(const BatchFillItem *__restrict__ items)
+{
+    const BatchFillItem I = items[blockIdx.y];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < I.n; i += (uint64_t)gridDim.x * blockDim.x)
+        I.dst[i] = I.value;
+}
+
+// ======================================================================================
 // launchers
 // ======================================================================================
 static inline unsigned stream_grid(uint64_t n, const DeviceInfo &dev)
@@ -686,6 +828,12 @@ cudaError_t prepare_device_kernels()
         e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
     }
+    void (*bfns[])(const BatchFwdItem *, int, uint32_t, uint32_t *) = {k_forward_batched<kStrict>,
+                                                                       k_forward_batched<kFast>};
+    for (auto f : bfns) {
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+    }
     if (dev < 64) g_attr_done[dev] = true;
     return cudaSuccess;
 }
@@ -739,9 +887,9 @@ template <int AR, bool LI, bool NS>
 static void dispatch_bwd_dt(int dt, dim3 grid, cudaStream_t s, float *vol, const void *ratio, const xpr_projdata *pd,
                             const LaunchArgs &a, int bx, int bz)
 {
-    if (dt == kBF16) k_backward_tiled<AR, LI, NS, kBF16><<<grid, NT, 0, s>>>(vol, ratio, pd, a, bx, bz);
-    else if (dt == kF16) k_backward_tiled<AR, LI, NS, kF16><<<grid, NT, 0, s>>>(vol, ratio, pd, a, bx, bz);
-    else k_backward_tiled<AR, LI, NS, kF32><<<grid, NT, 0, s>>>(vol, ratio, pd, a, bx, bz);
+    if (dt == kBF16) k_backward_tiled<AR, LI, NS, kBF16, BWD_BY><<<grid, NT, 0, s>>>(vol, ratio, pd, a, bx, bz);
+    else if (dt == kF16) k_backward_tiled<AR, LI, NS, kF16, BWD_BY><<<grid, NT, 0, s>>>(vol, ratio, pd, a, bx, bz);
+    else k_backward_tiled<AR, LI, NS, kF32, BWD_BY><<<grid, NT, 0, s>>>(vol, ratio, pd, a, bx, bz);
 }
 
 template <int AR, bool LI, bool NS>
@@ -870,6 +1018,114 @@ cudaError_t launch_convert(const float *src, void *dst, int dtype, uint64_t n, c
     if (dtype == kBF16) k_convert<kBF16><<<grid, 256, 0, s>>>(src, dst, n);
     else if (dtype == kF16) k_convert<kF16><<<grid, 256, 0, s>>>(src, dst, n);
     else return cudaMemcpyAsync(dst, src, n * 4, cudaMemcpyDeviceToDevice, s);
+    return cudaGetLastError();
+}
+
+// ---- batched launchers ---------------------------------------------------------------
+int forward_brick(int axis) { return axis == 0 ? BX : (axis == 1 ? BY : BZ); }
+int backward_brick(int axis, int cb) { return axis == 0 ? BX : (axis == 1 ? cb : BWD_BZ); }
+
+template <int AR, int DT>
+static void *bwd_batched_fn(int cb)
+{
+    return cb == 8 ? (void *)k_backward_batched<AR, DT, 8> : (void *)k_backward_batched<AR, DT, 16>;
+}
+
+static void *batched_fn(int kind, int arith, int dtype, int cb)
+{
+    if (kind == 0) return arith == kFast ? (void *)k_forward_batched<kFast> : (void *)k_forward_batched<kStrict>;
+    if (arith == kFast) {
+        if (dtype == kBF16) return bwd_batched_fn<kFast, kBF16>(cb);
+        if (dtype == kF16) return bwd_batched_fn<kFast, kF16>(cb);
+        return bwd_batched_fn<kFast, kF32>(cb);
+    }
+    if (dtype == kBF16) return bwd_batched_fn<kStrict, kBF16>(cb);
+    if (dtype == kF16) return bwd_batched_fn<kStrict, kF16>(cb);
+    return bwd_batched_fn<kStrict, kF32>(cb);
+}
+
+int batched_ctas_per_sm(int kind, int arith, int dtype, int cb)
+{
+    if (prepare_device_kernels() != cudaSuccess) return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batched_fn(kind, arith, dtype, cb), NT,
+                                                      kind == 0 ? kFwdSmem : 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+cudaError_t launch_forward_batched(const BatchFwdItem *items, int n_items, uint32_t total_units, uint32_t *ticket,
+                                   int arith, unsigned ctas, cudaStream_t s)
+{
+    cudaError_t e = prepare_device_kernels();
+    if (e != cudaSuccess) return e;
+    if (n_items <= 0 || total_units == 0) return cudaSuccess;
+    ctas = std::max(1u, std::min(ctas, total_units));
+    if (arith == kFast) k_forward_batched<kFast><<<ctas, NT, kFwdSmem, s>>>(items, n_items, total_units, ticket);
+    else k_forward_batched<kStrict><<<ctas, NT, kFwdSmem, s>>>(items, n_items, total_units, ticket);
+    return cudaGetLastError();
+}
+
+template <int AR, int DT>
+static void bwd_batched(int cb, unsigned ctas, cudaStream_t s, const BatchBwdItem *items, int n, uint32_t total,
+                        uint32_t *ticket)
+{
+    if (cb == 8) k_backward_batched<AR, DT, 8><<<ctas, NT, 0, s>>>(items, n, total, ticket);
+    else k_backward_batched<AR, DT, 16><<<ctas, NT, 0, s>>>(items, n, total, ticket);
+}
+
+cudaError_t launch_backward_batched(const BatchBwdItem *items, int n_items, uint32_t total_units, uint32_t *ticket,
+                                    int arith, int dt, int cb, unsigned ctas, cudaStream_t s)
+{
+    if (n_items <= 0 || total_units == 0) return cudaSuccess;
+    ctas = std::max(1u, std::min(ctas, total_units));
+    if (arith == kFast) {
+        if (dt == kBF16) bwd_batched<kFast, kBF16>(cb, ctas, s, items, n_items, total_units, ticket);
+        else if (dt == kF16) bwd_batched<kFast, kF16>(cb, ctas, s, items, n_items, total_units, ticket);
+        else bwd_batched<kFast, kF32>(cb, ctas, s, items, n_items, total_units, ticket);
+    } else {
+        if (dt == kBF16) bwd_batched<kStrict, kBF16>(cb, ctas, s, items, n_items, total_units, ticket);
+        else if (dt == kF16) bwd_batched<kStrict, kF16>(cb, ctas, s, items, n_items, total_units, ticket);
+        else bwd_batched<kStrict, kF32>(cb, ctas, s, items, n_items, total_units, ticket);
+    }
+    return cudaGetLastError();
+}
+
+template <int IDT>
+static void err_batched(int rdt, dim3 grid, cudaStream_t s, const BatchErrItem *items)
+{
+    if (rdt == kBF16) k_error_batched<IDT, kBF16><<<grid, 256, 0, s>>>(items);
+    else if (rdt == kF16) k_error_batched<IDT, kF16><<<grid, 256, 0, s>>>(items);
+    else k_error_batched<IDT, kF32><<<grid, 256, 0, s>>>(items);
+}
+
+static dim3 batched_stream_grid(int n_items, uint64_t max_n, const DeviceInfo &dev)
+{
+    const uint64_t want = (max_n + 255) / 256;
+    const uint64_t cap = std::max<uint64_t>(1, (uint64_t)dev.sm_count * 8 / (uint64_t)std::max(1, n_items));
+    return dim3((unsigned)std::max<uint64_t>(1, std::min(want, std::max<uint64_t>(cap, 4))), (unsigned)n_items);
+}
+
+cudaError_t launch_error_batched(const BatchErrItem *items, int n_items, int idt, int rdt, uint64_t max_n,
+                                 const DeviceInfo &dev, cudaStream_t s)
+{
+    if (n_items <= 0 || max_n == 0) return cudaSuccess;
+    if (n_items > 65535) return cudaErrorInvalidValue;
+    const dim3 grid = batched_stream_grid(n_items, max_n, dev);
+    if (idt == kBF16) err_batched<kBF16>(rdt, grid, s, items);
+    else if (idt == kF16) err_batched<kF16>(rdt, grid, s, items);
+    else err_batched<kF32>(rdt, grid, s, items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_batched(const BatchFillItem *items, int n_items, uint64_t max_n, const DeviceInfo &dev,
+                                cudaStream_t s)
+{
+    if (n_items <= 0 || max_n == 0) return cudaSuccess;
+    if (n_items > 65535) return cudaErrorInvalidValue;
+    k_fill_batched<<<batched_stream_grid(n_items, max_n, dev), 256, 0, s>>>(items);
     return cudaGetLastError();
 }
 
