@@ -33,6 +33,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cfloat>
 
 #include "xpr_internal.h"
@@ -63,7 +64,7 @@ struct __align__(16) ProjMeta {
     uint4 fast;                           // {kMagic + u0, u1 - u0, kMagic + v0, v1 - v0}
     int4 rect;                            // {u0, u1 - u0, v0, v1 - v0}
     uint4 tgt;                            // {pitch, off, img_base, tile width}
-    int4 flags;                           // {mode, lanes across z, column, v1 - v0 (rows)}
+    int4 flags;                           // {mode, lanes across z, column, inside (no bounds tests)}
 };
 
 // --------------------------------------------------------------------------------------
@@ -117,11 +118,18 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
         int r = min((int)ceilf(fminf(__ldg(vp + 1), 1.0e9f)), (int)a.det_w);
         int b = max((int)ceilf(fmaxf(__ldg(vp + 2), -1.0e9f)), 0);
         int t = min((int)ceilf(fminf(__ldg(vp + 3), 1.0e9f)), (int)a.rows);
+        // inside: the brick's whole footprint (corner projections with a margin of 2
+        // pixels, far above the rounding of any voxel's pixel) lies in the viewport, so
+        // every voxel of the brick lands in the rectangle and needs no bounds test
+        int inside = 0;
         if (ok) {
-            l = max(l, (int)floorf(umin) - 2);
-            r = min(r, (int)ceilf(umax) + 3);
-            b = max(b, (int)floorf(vmn) - 2);
-            t = min(t, (int)ceilf(vmx) + 3);
+            const int fl = (int)floorf(umin) - 2, fr = (int)ceilf(umax) + 3;
+            const int fb = (int)floorf(vmn) - 2, ft = (int)ceilf(vmx) + 3;
+            inside = fl >= l && fr <= r && fb >= b && ft <= t;
+            l = max(l, fl);
+            r = min(r, fr);
+            b = max(b, fb);
+            t = min(t, ft);
         }
         const int area = (r - l) * (t - b);
         const int mode = (!valid || r <= l || t <= b) ? kSkip : ((ok && area <= TILE_CAP) ? kTile : kDirect);
@@ -135,7 +143,7 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
         M.fast = make_uint4(kMagic + (uint32_t)l, (uint32_t)(r - l), kMagic + (uint32_t)b, (uint32_t)(t - b));
         M.rect = make_int4(l, r - l, b, t - b);
         M.tgt = make_uint4(pitch, off, img_base, (uint32_t)(r - l));
-        M.flags = make_int4(mode, fabsf(cw0) > fabsf(cw2), (cu1 == 0.0f) && (cw1 == 0.0f), t - b);
+        M.flags = make_int4(mode, fabsf(cw0) > fabsf(cw2), (cu1 == 0.0f) && (cw1 == 0.0f), inside);
     }
 }
 
@@ -170,13 +178,15 @@ __device__ __forceinline__ uint32_t fdist(float y, uint32_t base)
 }
 
 // Column walker.  For the voxel column (ax, az) and y-positions py[0..LEN), calls
-// f(k, in, idx) with idx the target index of ProjMeta.  Untilted projections
+// f(inside, k, in, idx) with idx the target index of ProjMeta.  Untilted projections
 // (flags.z) hoist u, w and 1/w out of the column; the others evaluate the full
-// contract per voxel.  Returns false, without calling f, when no column of the
-// warp meets the projection's u range.
+// contract per voxel.  In the FAST contract a brick whose footprint lies inside the
+// viewport (flags.w) skips the bounds tests: `inside` is then std::true_type and
+// `in` is true for every voxel.  Returns 0, without calling f, when no column of the
+// warp meets the projection's u range; 2 when the inside path ran; 1 otherwise.
 template <int ARITH, int LEN, typename F>
-__device__ __forceinline__ bool walk_column(const ProjMeta &M, const LaunchArgs &a, int ax, int az,
-                                            const float (&py)[LEN], F &&f)
+__device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &a, int ax, int az,
+                                           const float (&py)[LEN], F &&f)
 {
     const float4 cu = M.cu, cv = M.cv, cw = M.cw;
     const uint4 tgt = M.tgt;
@@ -187,17 +197,40 @@ __device__ __forceinline__ bool walk_column(const ProjMeta &M, const LaunchArgs 
         const uint4 fb = M.fast;
         const float Cu = col_fast(cu, px, pz), Cv = col_fast(cv, px, pz), Cw = col_fast(cw, px, pz);
         const float hv = a.half_minus_off;
+        if (M.flags.w) {
+            // dv = bits(fadd_rz(yv, 2^23)) - fb.z is in [0, rows) for every voxel, so the
+            // index dv * pitch + du + off is bits * pitch + (du + off - fb.z * pitch) mod 2^32
+            const uint32_t Kv = tgt.y - fb.z * pitch;
+            if (M.flags.z) {
+                const float rw = __frcp_rn(Cw);
+                const uint32_t K = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x) + Kv;
+                const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
+#pragma unroll
+                for (int k = 0; k < LEN; ++k)
+                    f(std::true_type{}, k, true,
+                      __float_as_uint(__fadd_rz(__fmaf_rn(py[k], Qv, Rv), 8388608.0f)) * pitch + K);
+            } else {
+#pragma unroll
+                for (int k = 0; k < LEN; ++k) {
+                    const float rw = __frcp_rn(__fmaf_rn(cw.y, py[k], Cw));
+                    const uint32_t du = fdist(__fmaf_rn(py[k], __fmul_rn(cu.y, rw), __fmaf_rn(Cu, rw, 0.5f)), fb.x);
+                    const float yv = __fmaf_rn(py[k], __fmul_rn(cv.y, rw), __fmaf_rn(Cv, rw, hv));
+                    f(std::true_type{}, k, true, __float_as_uint(__fadd_rz(yv, 8388608.0f)) * pitch + du + Kv);
+                }
+            }
+            return 2;
+        }
         if (M.flags.z) {
             const float rw = __frcp_rn(Cw);
             const uint32_t du = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x);
             const bool in_u = du < fb.y;
-            if (!__any_sync(0xffffffffu, in_u)) return false;
+            if (!__any_sync(0xffffffffu, in_u)) return 0;
             const uint32_t K = du + tgt.y;
             const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
                 const uint32_t dv = fdist(__fmaf_rn(py[k], Qv, Rv), fb.z);
-                f(k, in_u && (dv < fb.w), dv * pitch + K);
+                f(std::false_type{}, k, in_u && (dv < fb.w), dv * pitch + K);
             }
         } else {
 #pragma unroll
@@ -205,7 +238,7 @@ __device__ __forceinline__ bool walk_column(const ProjMeta &M, const LaunchArgs 
                 const float rw = __frcp_rn(__fmaf_rn(cw.y, py[k], Cw));
                 const uint32_t du = fdist(__fmaf_rn(py[k], __fmul_rn(cu.y, rw), __fmaf_rn(Cu, rw, 0.5f)), fb.x);
                 const uint32_t dv = fdist(__fmaf_rn(py[k], __fmul_rn(cv.y, rw), __fmaf_rn(Cv, rw, hv)), fb.z);
-                f(k, (du < fb.y) && (dv < fb.w), dv * pitch + du + tgt.y);
+                f(std::false_type{}, k, (du < fb.y) && (dv < fb.w), dv * pitch + du + tgt.y);
             }
         }
     } else {
@@ -219,14 +252,14 @@ __device__ __forceinline__ bool walk_column(const ProjMeta &M, const LaunchArgs 
             const float nw = num_strict(cw, px, 0.0f, pz);
             const uint32_t du = (uint32_t)(__float2int_rz(roundf(__fdiv_rn(nu, nw))) - rc.x);
             const bool in_u = du < (uint32_t)rc.y;
-            if (!__any_sync(0xffffffffu, in_u)) return false;
+            if (!__any_sync(0xffffffffu, in_u)) return 0;
             const uint32_t K = du + tgt.y;
             const float Pv = __fmul_rn(cv.x, px), Rv = __fmul_rn(cv.z, pz);
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
                 const float nv = __fadd_rn(__fadd_rn(__fadd_rn(Pv, __fmul_rn(cv.y, py[k])), Rv), cv.w);
                 const uint32_t dv = (uint32_t)(__float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off))) - rc.z);
-                f(k, in_u && (dv < (uint32_t)rc.w), dv * pitch + K);
+                f(std::false_type{}, k, in_u && (dv < (uint32_t)rc.w), dv * pitch + K);
             }
         } else {
 #pragma unroll
@@ -236,11 +269,11 @@ __device__ __forceinline__ bool walk_column(const ProjMeta &M, const LaunchArgs 
                 const float nw = num_strict(cw, px, py[k], pz);
                 const uint32_t du = (uint32_t)(__float2int_rz(roundf(__fdiv_rn(nu, nw))) - rc.x);
                 const uint32_t dv = (uint32_t)(__float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off))) - rc.z);
-                f(k, (du < (uint32_t)rc.y) && (dv < (uint32_t)rc.w), dv * pitch + du + tgt.y);
+                f(std::false_type{}, k, (du < (uint32_t)rc.y) && (dv < (uint32_t)rc.w), dv * pitch + du + tgt.y);
             }
         }
     }
-    return true;
+    return 1;
 }
 
 // --------------------------------------------------------------------------------------
@@ -306,12 +339,13 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 const uint32_t *vals = s_val + cz * VSTRIDE + cx;
                 const int ax = a.vmin[0] + x0 + cx, az = a.vmin[2] + z0 + cz;
                 if (fl.x == kTile) {
-                    walk_column<ARITH, BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
+                    // a zero adds nothing to a shared-memory tile; no test for it
+                    walk_column<ARITH, BY>(M, a, ax, az, py, [&](auto, int k, bool in, uint32_t idx) {
                         const uint32_t v = vals[k * BZ * VSTRIDE];
-                        if (in & (v != 0u)) atomicAdd(&tile[idx], v);
+                        if (in) atomicAdd(&tile[idx], v);
                     });
                 } else {
-                    walk_column<ARITH, BY>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
+                    walk_column<ARITH, BY>(M, a, ax, az, py, [&](auto, int k, bool in, uint32_t idx) {
                         const uint32_t v = vals[k * BZ * VSTRIDE];
                         if (in & (v != 0u)) atomicAdd(&sum[idx], v);
                     });
@@ -423,12 +457,21 @@ __global__ void k_pad_items(float *vol, uint32_t *sum, const void *ratio, const 
 // --------------------------------------------------------------------------------------
 // backward
 // --------------------------------------------------------------------------------------
+// The stored bits of ratio element i (zero-extended for the 16-bit types) and their
+// value: a gather returns raw bits so that an out-of-bounds pair can keep 0 (the bits
+// of +0.0 in every type) without a select after the conversion.
 template <int DT>
-__device__ __forceinline__ float load_ratio(const void *ratio, uint32_t i)
+__device__ __forceinline__ uint32_t load_ratio_bits(const void *ratio, uint32_t i)
 {
-    if (DT == kF32) return __ldg((const float *)ratio + i);
-    if (DT == kBF16) return __bfloat162float(__ldg((const __nv_bfloat16 *)ratio + i));
-    return __half2float(__ldg((const __half *)ratio + i));
+    if (DT == kF32) return __float_as_uint(__ldg((const float *)ratio + i));
+    return (uint32_t)__ldg((const unsigned short *)ratio + i);
+}
+template <int DT>
+__device__ __forceinline__ float ratio_from_bits(uint32_t b)
+{
+    if (DT == kF32) return __uint_as_float(b);
+    if (DT == kBF16) return __uint_as_float(b << 16);  // bf16 is the high half of an f32
+    return __half2float(__ushort_as_half((unsigned short)b));
 }
 
 // One backward work unit: the brick of 32 x CB x 8 voxels `brick` (x fastest, then z,
@@ -451,6 +494,7 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
 
     float py[CB], s[CB];
     uint32_t n2[CB / 2];  // in-bounds counts, two 16-bit halves per word (k even: low, odd: high)
+    uint32_t n_inside = 0;  // projections walked on the inside path: every voxel of the column counted
 #pragma unroll
     for (int k = 0; k < CB; ++k) {
         py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
@@ -470,13 +514,17 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
             // the column's gathers are issued before any is consumed (all in flight together);
             // an out-of-bounds pair contributes r = 0, and s + 0 == s exactly (s is never -0)
             float r[CB];
-            const bool walked = walk_column<ARITH, CB>(M, a, ax, az, py, [&](int k, bool in, uint32_t idx) {
-                r[k] = 0.0f;
-                if (in) r[k] = load_ratio<DT>(ratio, idx);
-                if (!NANSKIP && in) n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
-                if (NANSKIP && !in) r[k] = __int_as_float(0x7fc00000);
+            const int walked = walk_column<ARITH, CB>(M, a, ax, az, py, [&](auto inside, int k, bool in, uint32_t idx) {
+                uint32_t bits = 0u;
+                if (in) bits = load_ratio_bits<DT>(ratio, idx);
+                r[k] = ratio_from_bits<DT>(bits);
+                if constexpr (!decltype(inside)::value) {
+                    if (!NANSKIP && in) n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
+                    if (NANSKIP && !in) r[k] = __int_as_float(0x7fc00000);
+                }
             });
             if (!walked) continue;  // warp-uniform
+            if (!NANSKIP && walked == 2) ++n_inside;
 #pragma unroll
             for (int k = 0; k < CB; ++k) {
                 if (NANSKIP) {
@@ -498,7 +546,7 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
     for (int k = 0; k < CB; ++k) {
         const int y = y0 + k;
         if (y < sy) {
-            const uint32_t cnt = (k & 1) ? (n2[k >> 1] >> 16) : (n2[k >> 1] & 0xffffu);
+            const uint32_t cnt = ((k & 1) ? (n2[k >> 1] >> 16) : (n2[k >> 1] & 0xffffu)) + n_inside;
             float *p = vol + ((size_t)y * sz + z) * sx + x;
             *p = __fmul_rn(*p, p_expf(__fdiv_rn(s[k], __uint2float_rn(cnt))));
         }
