@@ -51,6 +51,10 @@ CONFIGS = {
                     "it=2, BF16 image/ratio storage, one batched persistent launch per phase in a CUDA graph",
                batch=64, dwidth=384, dheight=384, projections=360, sit=10, it=2, modules=3, px=0.1, rpy=2.0,
                phantom=256, ellipsoids=12, background=0.0, i0=1e5, seed=4, plain_sample=4),
+    # one problem of the c4 family (profiling-sized)
+    "c4one": dict(desc="one 384^3 recon grid of the c4 family (3 tilted modules, 36 projections per sub-iteration)",
+                  batch=1, dwidth=384, dheight=384, projections=360, sit=10, it=2, modules=3, px=0.1, rpy=2.0,
+                  phantom=256, ellipsoids=12, background=0.0, i0=1e5, seed=4, plain_sample=0),
 }
 
 FLOPS_PER_PAIR = 44          # algorithmic FP32 operations per (voxel, projection) pair, forward + backward
@@ -68,7 +72,8 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--arith", choices=["fast", "strict"], default="fast")
-    p.add_argument("--storage", choices=["fp32", "bf16", "fp16"], default="fp32")
+    p.add_argument("--storage", choices=["fp32", "bf16", "fp16"], default=None,
+                   help="image / ratio storage (default: fp32; bf16 for the batched configurations)")
     p.add_argument("--config", choices=sorted(CONFIGS), default="c2")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
@@ -402,6 +407,7 @@ def run_ours(args, cfg, rank, world, local):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    args.storage = args.storage or "fp32"
     prob = Problem(cfg, args.arith, args.storage, local, cfg["seed"] + 1000 * rank)
     stream = prob.stream
     K, Wm = args.steps, args.warmup
@@ -558,8 +564,7 @@ def run_batched(args, cfg, rank, world, local):
     L = _lib.lib()
     ctx = Context(local)
     rng = np.random.default_rng(cfg["seed"] + 1000 * rank)
-    storage = {"fp32": _lib.F32, "bf16": _lib.BF16, "fp16": _lib.F16}[args.storage if args.storage != "fp32"
-                                                                       else "bf16"]
+    storage = {"fp32": _lib.F32, "bf16": _lib.BF16, "fp16": _lib.F16}[args.storage or "bf16"]
     S, it, M, P = cfg["sit"], cfg["it"], cfg["modules"], cfg["projections"]
     Wd, Hd = cfg["dwidth"], cfg["dheight"]
     stream = torch.cuda.current_stream()

@@ -466,6 +466,10 @@ __device__ __forceinline__ uint32_t load_ratio_bits(const void *ratio, uint32_t 
     if (DT == kF32) return __float_as_uint(__ldg((const float *)ratio + i));
     return (uint32_t)__ldg((const unsigned short *)ratio + i);
 }
+// a quiet NaN in each storage type's bits
+template <int DT>
+constexpr uint32_t kNaNBits = DT == kF32 ? 0x7fc00000u : (DT == kBF16 ? 0x7fc0u : 0x7e00u);
+
 template <int DT>
 __device__ __forceinline__ float ratio_from_bits(uint32_t b)
 {
@@ -503,37 +507,44 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
 #pragma unroll
     for (int k = 0; k < CB / 2; ++k) n2[k] = 0u;
 
-    for (int e0 = 0; e0 < (int)a.n_entries; e0 += G) {
-        if (warp == 0)
-            compute_meta<LIST, true>(s_meta, pd, a, e0, (int)a.n_entries, x0, y0, z0, BX, CB, BWD_BZ, lane);
-        __syncthreads();
+    // metadata double buffer (s_meta holds 2 * G entries): warp 0 prepares the next group
+    // while the CTA walks the current one, so one barrier per group suffices
+    const int n_entries = (int)a.n_entries;
+    if (warp == 0) compute_meta<LIST, true>(s_meta, pd, a, 0, n_entries, x0, y0, z0, BX, CB, BWD_BZ, lane);
+    __syncthreads();
+    for (int e0 = 0, buf = 0; e0 < n_entries; e0 += G, buf ^= G) {
+        if (warp == 0 && e0 + G < n_entries)
+            compute_meta<LIST, true>(s_meta + (buf ^ G), pd, a, e0 + G, n_entries, x0, y0, z0, BX, CB, BWD_BZ,
+                                     lane);
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
-            const ProjMeta &M = s_meta[g];
+            const ProjMeta &M = s_meta[buf + g];
             if (M.flags.x == kSkip) continue;
             // the column's gathers are issued before any is consumed (all in flight together);
-            // an out-of-bounds pair contributes r = 0, and s + 0 == s exactly (s is never -0)
-            float r[CB];
+            // an out-of-bounds pair contributes r = 0, and s + 0 == s exactly (s is never -0).
+            // Raw bits first, values after: the loads of the column stay independent of
+            // any conversion, so they are all in flight together in every storage type.
+            uint32_t rb[CB];
             const int walked = walk_column<ARITH, CB>(M, a, ax, az, py, [&](auto inside, int k, bool in, uint32_t idx) {
-                uint32_t bits = 0u;
-                if (in) bits = load_ratio_bits<DT>(ratio, idx);
-                r[k] = ratio_from_bits<DT>(bits);
+                rb[k] = 0u;
+                if (in) rb[k] = load_ratio_bits<DT>(ratio, idx);
                 if constexpr (!decltype(inside)::value) {
                     if (!NANSKIP && in) n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
-                    if (NANSKIP && !in) r[k] = __int_as_float(0x7fc00000);
+                    if (NANSKIP && !in) rb[k] = kNaNBits<DT>;
                 }
             });
             if (!walked) continue;  // warp-uniform
             if (!NANSKIP && walked == 2) ++n_inside;
 #pragma unroll
             for (int k = 0; k < CB; ++k) {
+                const float r = ratio_from_bits<DT>(rb[k]);
                 if (NANSKIP) {
-                    if (r[k] == r[k]) {
-                        s[k] = __fadd_rn(s[k], r[k]);
+                    if (r == r) {
+                        s[k] = __fadd_rn(s[k], r);
                         n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
                     }
                 } else {
-                    s[k] = __fadd_rn(s[k], r[k]);
+                    s[k] = __fadd_rn(s[k], r);
                 }
             }
         }
@@ -559,7 +570,7 @@ __global__ void __launch_bounds__(NT, 3)
     k_backward_tiled(float *__restrict__ vol, const void *__restrict__ ratio, const xpr_projdata *__restrict__ pd,
                      const LaunchArgs a, int bricks_x, int bricks_z)
 {
-    __shared__ ProjMeta s_meta[G];
+    __shared__ ProjMeta s_meta[2 * G];
     backward_unit<ARITH, LIST, NANSKIP, DT, CB>(vol, ratio, pd, a, blockIdx.x, bricks_x, bricks_z, s_meta);
 }
 
@@ -752,7 +763,7 @@ template <int ARITH, int DT, int CB>
 __global__ void __launch_bounds__(NT, 3)
     k_backward_batched(const BatchBwdItem *__restrict__ items, int n_items, uint32_t total_units, uint32_t *ticket)
 {
-    __shared__ ProjMeta s_meta[G];
+    __shared__ ProjMeta s_meta[2 * G];
     __shared__ LaunchArgs s_a;
     __shared__ uint32_t s_unit;
     __shared__ int s_item;
