@@ -326,7 +326,9 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
         __syncthreads();
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
-            const ProjMeta &M = s_meta[g];
+            // a register copy: the walk's shared-memory atomics would otherwise force the
+            // metadata to be re-read from shared memory for every column
+            const ProjMeta M = s_meta[g];
             const int4 fl = M.flags;
             if (fl.x == kSkip) continue;
             uint32_t *tile = s_tile + g * TILE_CAP;
