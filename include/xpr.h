@@ -219,6 +219,61 @@ int xpr_batch_schedule(const xpr_batch *b, int32_t *fwd_splits, int32_t *bwd_col
                        double *tuned_ms);
 int xpr_batch_destroy(xpr_batch *b);
 
+/* ---------------------------------------------------------------- serving */
+/* A request loop with continuous batching.  Each request is a naive reconstruction
+ * (reconstruction_n.hpp:27-88) of raw projections held by the caller, with its
+ * parameters in the XPRecon JSON schema (recon / geometry / detector; the detector size
+ * and projection count come from the images).  A request is admitted when the device
+ * memory it needs fits the server's budget (first come, first served); it then joins
+ * the running batch at the next sub-iteration boundary and every active request advances
+ * one sub-iteration per tick (one persistent forward, error and backward launch over all
+ * of them).  Its volume, images and scratch stay resident until its last sub-iteration;
+ * the volume is then copied to the caller's buffer and the memory freed.  Uploads and
+ * downloads run on their own streams beside the compute.  A request's result is
+ * bit-identical whatever else is being served (see xpr_batch).  No counterpart in the
+ * reference.  recon.seed should be set: without it the jitter seed is random, as in the
+ * reference. */
+typedef struct xpr_serve_opts {
+    int32_t arith;                /* xpr_arith for every request */
+    int32_t storage;              /* xpr_dtype of the images and ratios of every request */
+    uint64_t mem_budget;          /* device bytes for resident requests; 0: 90% of the free memory */
+    uint32_t max_active;          /* requests resident at once; 0: no limit */
+} xpr_serve_opts;
+
+enum xpr_request_state { XPR_REQ_QUEUED = 0, XPR_REQ_ACTIVE = 1, XPR_REQ_DONE = 2, XPR_REQ_FAILED = 3 };
+
+typedef struct xpr_request_info {
+    int32_t state;                /* xpr_request_state */
+    int32_t error;                /* XPR_ERR_* of a failed request */
+    double submit_s, admit_s, done_s;  /* seconds since the server started */
+    uint64_t pairs;               /* voxel x projection pairs of the whole reconstruction */
+    uint64_t device_bytes;        /* device memory held while resident */
+} xpr_request_info;
+
+typedef struct xpr_serve_stats {
+    uint64_t submitted, completed, failed;
+    uint64_t ticks;               /* batched sub-iteration steps launched */
+    uint64_t pairs;               /* voxel x projection pairs processed */
+    uint32_t active, queued;
+    uint64_t bytes_in_use, peak_bytes;
+} xpr_serve_stats;
+
+typedef struct xpr_server xpr_server;
+int xpr_serve_create(xpr_ctx *ctx, const xpr_serve_opts *opts, xpr_server **out);
+/* raw: count images of height x width float32 intensities in acquisition order, read by
+ * the server until the request completes; vol_out: host memory for vwidth * vheight *
+ * vwidth floats, written before the request is reported done.  Malformed parameters or a
+ * request larger than the whole budget fail here (XPR_ERR_PARAM / XPR_ERR_CAP). */
+int xpr_serve_submit(xpr_server *s, const char *json, const float *raw, int64_t count, uint32_t width,
+                     uint32_t height, float *vol_out, uint64_t vol_cap, uint64_t *ticket);
+int xpr_serve_poll(xpr_server *s, uint64_t ticket, xpr_request_info *info);
+/* Blocks until the request is done or failed, or timeout_s (< 0: no limit) passes;
+ * returns XPR_OK with info->state set either way. */
+int xpr_serve_wait(xpr_server *s, uint64_t ticket, double timeout_s, xpr_request_info *info);
+int xpr_serve_stats_get(xpr_server *s, xpr_serve_stats *stats);
+/* Waits for every submitted request, then stops the server and frees its resources. */
+int xpr_serve_destroy(xpr_server *s);
+
 /* ---------------------------------------------------------------- geometry (host) */
 /* Geometry parameters (global_parameters.hpp:23-54, parameters.hpp:34-48). */
 typedef struct xpr_geom_params {

@@ -21,14 +21,11 @@
 #include <tuple>
 #include <vector>
 
-#include "../xpr_internal.h"
-#include "xpr.h"
+#include "batch_plan.h"
 
 namespace {
 
 constexpr uint32_t kOneBits = 0x3f800000u;  // 1.0f
-
-size_t dtype_size(int dt) { return dt == XPR_F32 ? 4 : 2; }
 
 struct StepPlan {
     size_t fwd_off = 0, err_off = 0, bwd_off = 0;  // byte offsets in the work-list buffer
@@ -47,14 +44,9 @@ std::map<ShapeKey, std::tuple<int, int, double>> g_tuned;
 struct xpr_batch {
     xpr_ctx *ctx = nullptr;
     const xpr::DeviceInfo *di = nullptr;
-    std::vector<xpr_batch_problem> probs;
+    std::vector<xpr::PlannedProblem> probs;
     xpr_batch_opts opts{};
     uint32_t steps = 0;
-    // per problem: origins (3 per step) and weights (1 per step)
-    std::vector<std::vector<float>> origin, weight;
-    std::vector<xpr::LaunchArgs> base;     // launch args without origin / split
-    std::vector<uint32_t *> sums;
-    std::vector<void *> ratios;
     void *scratch = nullptr;               // sums and ratios of every problem
     uint32_t *tickets = nullptr;           // [0, 2): forward, [2, 4): backward
     void *lists = nullptr;                 // work lists of every step
@@ -78,10 +70,6 @@ int cuda_fail(cudaError_t e, const char *what)
     return xpr::set_last_error(XPR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
-
-uint32_t entries_of(const xpr_batch_problem &p) { return p.per_subset * (p.modules ? p.modules : 1u); }
-
 // persistent CTAs for a launch kind (0 forward, 1 backward): the occupancy limit per SM
 // (or the requested number below it) on every SM
 unsigned grid_of(const xpr_batch *b, int kind)
@@ -91,86 +79,32 @@ unsigned grid_of(const xpr_batch *b, int kind)
     return (unsigned)(b->di->sm_count * per_sm);
 }
 
-// per_split (entries per forward work unit, a multiple of the metadata group) for `splits`
-uint32_t per_split_for(uint32_t entries, int splits)
-{
-    const uint32_t g = 4;
-    return (uint32_t)div_up(div_up(entries, (uint64_t)std::max(1, splits)), g) * g;
-}
-
 int build_lists(xpr_batch *b, int splits, int column, cudaStream_t s)
 {
-    const int n = (int)b->probs.size();
     std::vector<char> host;
     b->plan.assign(b->steps, StepPlan{});
-    const int fbx = xpr::forward_brick(0), fby = xpr::forward_brick(1), fbz = xpr::forward_brick(2);
-    const int bbx = xpr::backward_brick(0, column), bby = xpr::backward_brick(1, column),
-              bbz = xpr::backward_brick(2, column);
     auto append = [&](const void *p, size_t bytes) {
         const size_t off = (host.size() + 15) & ~(size_t)15;
         host.resize(off + bytes);
         std::memcpy(host.data() + off, p, bytes);
         return off;
     };
+    xpr::StepItems it;
     for (uint32_t k = 0; k < b->steps; ++k) {
         StepPlan &P = b->plan[k];
-        std::vector<xpr::BatchFwdItem> fw;
-        std::vector<xpr::BatchErrItem> er;
-        std::vector<xpr::BatchBwdItem> bw;
-        for (int i = 0; i < n; ++i) {
-            const xpr_batch_problem &p = b->probs[i];
-            if (k >= p.it * p.sit) continue;
-            const uint32_t s_idx = k % p.sit;
-            const uint32_t E = entries_of(p);
-            xpr::LaunchArgs a = b->base[i];
-            for (int c = 0; c < 3; ++c) a.origin[c] = b->origin[i][3 * k + c];
-            const xpr_projdata *pd = p.projdata + (size_t)s_idx * E;
-            const uint64_t npix = (uint64_t)p.per_subset * p.det_w * p.det_h;
-            if (k > 0) {
-                xpr::BatchFwdItem f{};
-                f.a = a;
-                f.a.per_split = per_split_for(E, splits);
-                f.vol = p.vol;
-                f.sum = b->sums[i];
-                f.pd = pd;
-                f.bricks_x = (int)div_up(p.vwidth, fbx);
-                f.bricks_z = (int)div_up(p.vwidth, fbz);
-                f.splits = (uint32_t)div_up(E, f.a.per_split);
-                f.unit_begin = P.fwd_units;
-                const uint64_t units = (uint64_t)f.bricks_x * f.bricks_z * div_up(p.vheight, fby) * f.splits;
-                if (P.fwd_units + units >= (1ull << 31)) return fail(XPR_ERR_UNSUPPORTED, "batch step too large");
-                P.fwd_units += (uint32_t)units;
-                fw.push_back(f);
-            }
-            xpr::BatchErrItem e{};
-            e.images = (const char *)p.images + (size_t)s_idx * npix * dtype_size(b->opts.storage);
-            e.sum = b->sums[i];
-            e.ratio = b->ratios[i];
-            e.residual = p.residual ? p.residual + k : nullptr;
-            e.n = npix;
-            e.weight = b->weight[i][k];
-            e.first = k == 0;
-            P.max_n = std::max(P.max_n, npix);
-            er.push_back(e);
-            xpr::BatchBwdItem w{};
-            w.a = a;
-            w.vol = p.vol;
-            w.ratio = b->ratios[i];
-            w.pd = pd;
-            w.bricks_x = (int)div_up(p.vwidth, bbx);
-            w.bricks_z = (int)div_up(p.vwidth, bbz);
-            w.unit_begin = P.bwd_units;
-            const uint64_t units = (uint64_t)w.bricks_x * w.bricks_z * div_up(p.vheight, bby);
-            if (P.bwd_units + units >= (1ull << 31)) return fail(XPR_ERR_UNSUPPORTED, "batch step too large");
-            P.bwd_units += (uint32_t)units;
-            bw.push_back(w);
-        }
-        P.n_fwd = (int)fw.size();
-        P.n_err = (int)er.size();
-        P.n_bwd = (int)bw.size();
-        if (!fw.empty()) P.fwd_off = append(fw.data(), fw.size() * sizeof(fw[0]));
-        if (!er.empty()) P.err_off = append(er.data(), er.size() * sizeof(er[0]));
-        if (!bw.empty()) P.bwd_off = append(bw.data(), bw.size() * sizeof(bw[0]));
+        it.clear();
+        for (const auto &pp : b->probs)
+            if (k < pp.steps() && !xpr::add_step_items(pp, k, splits, column, b->opts.storage, &it))
+                return fail(XPR_ERR_UNSUPPORTED, "batch step exceeds 2^31 work units");
+        P.n_fwd = (int)it.fwd.size();
+        P.n_err = (int)it.err.size();
+        P.n_bwd = (int)it.bwd.size();
+        P.fwd_units = it.fwd_units;
+        P.bwd_units = it.bwd_units;
+        P.max_n = it.max_n;
+        if (!it.fwd.empty()) P.fwd_off = append(it.fwd.data(), it.fwd.size() * sizeof(it.fwd[0]));
+        if (!it.err.empty()) P.err_off = append(it.err.data(), it.err.size() * sizeof(it.err[0]));
+        if (!it.bwd.empty()) P.bwd_off = append(it.bwd.data(), it.bwd.size() * sizeof(it.bwd[0]));
     }
     if (host.size() > b->lists_bytes) {
         if (b->lists) xpr_free(b->ctx, b->lists);
@@ -273,8 +207,9 @@ int autotune(xpr_batch *b, cudaStream_t s)
 {
     uint32_t max_e = 0;
     std::vector<uint64_t> shape;
-    for (const auto &p : b->probs) {
-        max_e = std::max(max_e, entries_of(p));
+    for (const auto &pp : b->probs) {
+        const xpr_batch_problem &p = pp.p;
+        max_e = std::max(max_e, xpr::entries_of(p));
         shape.insert(shape.end(), {p.vwidth, p.vheight, p.det_w, p.det_h, p.per_subset, p.modules});
     }
     const ShapeKey key{b->opts.arith, b->opts.storage, shape};
@@ -291,7 +226,7 @@ int autotune(xpr_batch *b, cudaStream_t s)
     if (b->steps > 1) {
         bool first = true;
         for (int sp : {1, 2, 4, 8, 16}) {
-            if (sp > 1 && (uint32_t)sp > div_up(max_e, 4)) break;
+            if (sp > 1 && (uint32_t)sp > xpr::div_up(max_e, 4)) break;
             if (int rc = build_lists(b, sp, b->column, s)) return rc;
             const float ms = time_ms(s, [&] {
                 enqueue_forward(b, 1, s);
@@ -363,60 +298,26 @@ int xpr_batch_create(xpr_ctx *ctx, const xpr_batch_problem *problems, uint32_t n
     b->ctx = ctx;
     b->di = di;
     b->opts = o;
-    b->probs.assign(problems, problems + n);
     b->ctas = o.ctas_per_sm;
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     uint64_t scratch_bytes = 0;
     uint64_t total_bricks = 0;
     uint32_t max_e = 0;
+    b->probs.resize(n);
     for (uint32_t i = 0; i < n; ++i) {
-        const xpr_batch_problem &p = b->probs[i];
-        if (!p.vol || !p.images || !p.projdata) {
-            release(b);
-            return fail(XPR_ERR_INVALID, "xpr_batch_create: NULL buffer in a problem");
-        }
-        if (p.sit == 0 || p.it == 0 || p.per_subset == 0 || p.vwidth == 0 || p.vheight == 0) {
-            release(b);
-            return fail(XPR_ERR_INVALID, "xpr_batch_create: sit, it, per_subset and the grid must be positive");
-        }
-        xpr_launch L{};
-        L.vmax[0] = (int32_t)p.vwidth;
-        L.vmax[1] = (int32_t)p.vheight;
-        L.vmax[2] = (int32_t)p.vwidth;
-        for (int c = 0; c < 3; ++c) {
-            L.origin[c] = p.orig[c];
-            L.voxel[c] = p.voxel;
-        }
-        L.det_w = p.det_w;
-        L.rows = p.det_h;
-        L.n_angles = p.per_subset;
-        L.modules = p.modules ? p.modules : 1u;
-        L.arith = o.arith;
-        xpr::LaunchArgs a;
-        if (const char *m = xpr::make_launch_args(&L, entries_of(p), &a)) {
+        const xpr_batch_problem &p = problems[i];
+        if (const char *m = xpr::plan_problem(p, o.arith, &b->probs[i])) {
             release(b);
             return xpr::set_last_error(XPR_ERR_INVALID, "xpr_batch_create: problem %u: %s", i, m);
         }
-        b->base.push_back(a);
         b->steps = std::max(b->steps, p.it * p.sit);
-        // jitter: 3 draws per sub-iteration from std::mt19937(seed) (reconstruction.hpp:268-272)
-        std::vector<float> jit((size_t)3 * p.it * p.sit), org(jit.size()), w((size_t)p.it * p.sit);
-        xpr_jitter(p.seed, jit.size(), p.voxel, jit.data());
-        float wt = p.weight;
-        for (uint32_t k = 0; k < p.it * p.sit; ++k) {
-            for (int c = 0; c < 3; ++c) org[3 * k + c] = p.orig[c] + jit[3 * k + c];
-            w[k] = wt;
-            if (k % p.sit == p.sit - 1) wt *= p.weight_factor;
-        }
-        b->origin.push_back(org);
-        b->weight.push_back(w);
-        const uint64_t npix = (uint64_t)p.per_subset * p.det_w * p.det_h;
-        scratch_bytes += ((npix * 4 + 255) & ~255ull) + ((npix * dtype_size(o.storage) + 255) & ~255ull);
+        const uint64_t npix = b->probs[i].npix();
+        scratch_bytes += ((npix * 4 + 255) & ~255ull) + ((npix * xpr::dtype_size(o.storage) + 255) & ~255ull);
         b->max_vol = std::max<uint64_t>(b->max_vol, (uint64_t)p.vwidth * p.vheight * p.vwidth);
         b->max_pix = std::max(b->max_pix, npix);
-        b->max_ratio_words = std::max<uint64_t>(b->max_ratio_words, div_up(npix * dtype_size(o.storage), 4));
-        total_bricks += div_up(p.vwidth, 32) * div_up(p.vwidth, 32) * div_up(p.vheight, 8);
-        max_e = std::max(max_e, entries_of(p));
+        b->max_ratio_words = std::max<uint64_t>(b->max_ratio_words, xpr::div_up(npix * xpr::dtype_size(o.storage), 4));
+        total_bricks += xpr::div_up(p.vwidth, 32) * xpr::div_up(p.vwidth, 32) * xpr::div_up(p.vheight, 8);
+        max_e = std::max(max_e, xpr::entries_of(p));
     }
     scratch_bytes += 256 + 3 * sizeof(xpr::BatchFillItem) * n;
     if (int rc = xpr_alloc(ctx, scratch_bytes, &b->scratch)) {
@@ -430,15 +331,16 @@ int xpr_batch_create(xpr_ctx *ctx, const xpr_batch_problem *problems, uint32_t n
     q += ((3 * sizeof(xpr::BatchFillItem) * n + 255) & ~(size_t)255);
     std::vector<xpr::BatchFillItem> fills(3 * (size_t)n);
     for (uint32_t i = 0; i < n; ++i) {
-        const xpr_batch_problem &p = b->probs[i];
-        const uint64_t npix = (uint64_t)p.per_subset * p.det_w * p.det_h;
-        b->sums.push_back((uint32_t *)q);
+        xpr::PlannedProblem &pp = b->probs[i];
+        const xpr_batch_problem &p = pp.p;
+        const uint64_t npix = pp.npix();
+        pp.sums = (uint32_t *)q;
         q += (npix * 4 + 255) & ~255ull;
-        b->ratios.push_back(q);
-        q += (npix * dtype_size(o.storage) + 255) & ~255ull;
+        pp.ratio = q;
+        q += (npix * xpr::dtype_size(o.storage) + 255) & ~255ull;
         fills[i] = {(uint32_t *)p.vol, (uint64_t)p.vwidth * p.vheight * p.vwidth, kOneBits, 0};
-        fills[n + i] = {b->sums[i], npix, 0u, 0};
-        fills[2 * n + i] = {(uint32_t *)b->ratios[i], div_up(npix * dtype_size(o.storage), 4), 0u, 0};
+        fills[n + i] = {pp.sums, npix, 0u, 0};
+        fills[2 * n + i] = {(uint32_t *)pp.ratio, xpr::div_up(npix * xpr::dtype_size(o.storage), 4), 0u, 0};
     }
     if ((e = cudaMemsetAsync(b->tickets, 0, 256, s)) != cudaSuccess ||
         (e = cudaMemcpyAsync(b->fills, fills.data(), fills.size() * sizeof(fills[0]), cudaMemcpyHostToDevice, s)) !=
@@ -452,7 +354,9 @@ int xpr_batch_create(xpr_ctx *ctx, const xpr_batch_problem *problems, uint32_t n
     int splits = o.fwd_splits;
     if (splits <= 0) {
         const uint64_t target = (uint64_t)di->sm_count * 4 * 3;
-        splits = total_bricks >= target ? 1 : (int)std::min<uint64_t>(div_up(target, total_bricks), div_up(max_e, 4));
+        splits = total_bricks >= target
+                     ? 1
+                     : (int)std::min<uint64_t>(xpr::div_up(target, total_bricks), xpr::div_up(max_e, 4));
         splits = std::max(splits, 1);
     }
     const int column = o.bwd_column ? o.bwd_column : 16;

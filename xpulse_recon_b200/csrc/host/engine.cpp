@@ -311,22 +311,7 @@ Engine::Engine(const Params &p, std::unique_ptr<ImageSource> images, bool write_
     d.M = p.module_number;
     if (!p.angle_list.empty() && (int64_t)p.angle_list.size() != d.P)
         throw std::runtime_error("The size of the angle list is different from the number of projections");
-    gp_.so = p.so; gp_.sd = p.sd; gp_.angle = p.angle; gp_.heli_offset = p.heli_offset;
-    gp_.px = p.px; gp_.rx_px = p.rx; gp_.sx = p.sx; gp_.sy = p.sy;
-    gp_.module_number = p.module_number;
-    gp_.module_angle_offset_set = p.module_angle_offset_set ? 1 : 0;
-    gp_.module_angle_offset = p.module_angle_offset;
-    gp_.module_center_offset_z = p.module_center_offset_z;
-    gp_.dwidth = d.Wd; gp_.dheight = d.Hd; gp_.projections = d.P; gp_.sit = d.S;
-    gp_.angle_list = p.angle_list.empty() ? nullptr : p.angle_list.data();
-    if (!p.modules.empty()) {
-        for (const auto &m : p.modules) {
-            d.mod_offset.insert(d.mod_offset.end(), {m.offset_x, m.offset_y, m.offset_z});
-            d.mod_rpy.insert(d.mod_rpy.end(), {m.roll, m.pitch, m.yaw});
-        }
-        gp_.mod_offset = d.mod_offset.data();
-        gp_.mod_rpy = d.mod_rpy.data();
-    }
+    geom_params_from(p, d.P, d.Wd, d.Hd, &gp_, &d.mod_offset, &d.mod_rpy);
     d.pd_all.resize((size_t)(d.P * d.M));
     check(xpr_geometry(&gp_, p.geometry == "fp64" ? 1 : 0, d.pd_all.data(), &go_), "geometry");
     d.Pc = go_.concurrent;

@@ -236,4 +236,37 @@ std::string params_to_json(const Params &p)
     return o.str();
 }
 
+void geom_params_from(const Params &p, int64_t projections, uint32_t width, uint32_t height,
+                      xpr_geom_params *gp, std::vector<float> *mod_offset, std::vector<float> *mod_rpy)
+{
+    *gp = xpr_geom_params{};
+    gp->so = p.so;
+    gp->sd = p.sd;
+    gp->angle = p.angle;
+    gp->heli_offset = p.heli_offset;
+    gp->px = p.px;
+    gp->rx_px = p.rx;
+    gp->sx = p.sx;
+    gp->sy = p.sy;
+    gp->module_number = p.module_number;
+    gp->module_angle_offset_set = p.module_angle_offset_set ? 1 : 0;
+    gp->module_angle_offset = p.module_angle_offset;
+    gp->module_center_offset_z = p.module_center_offset_z;
+    gp->dwidth = width;
+    gp->dheight = height;
+    gp->projections = projections;
+    gp->sit = p.sit;
+    gp->angle_list = p.angle_list.empty() ? nullptr : p.angle_list.data();
+    mod_offset->clear();
+    mod_rpy->clear();
+    if (!p.modules.empty()) {
+        for (const auto &m : p.modules) {
+            mod_offset->insert(mod_offset->end(), {m.offset_x, m.offset_y, m.offset_z});
+            mod_rpy->insert(mod_rpy->end(), {m.roll, m.pitch, m.yaw});
+        }
+        gp->mod_offset = mod_offset->data();
+        gp->mod_rpy = mod_rpy->data();
+    }
+}
+
 }  // namespace xpr

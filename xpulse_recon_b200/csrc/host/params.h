@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "../../../include/xpr.h"
 #include "json.h"
 
 namespace xpr {
@@ -86,5 +87,11 @@ Params params_from_json(const json::Value &root);
 // The default parameter set serialised as JSON (XPRecon -template, main.cpp:75-79).
 std::string params_to_json(const Params &p);
 uint64_t parse_bytes(const std::string &s);
+
+// The geometry parameters of `p` for `projections` images of width x height
+// (dataset.hpp:214-235 derives dwidth / dheight / projections from the images).
+// mod_offset / mod_rpy receive the per-module arrays gp points into.
+void geom_params_from(const Params &p, int64_t projections, uint32_t width, uint32_t height,
+                      xpr_geom_params *gp, std::vector<float> *mod_offset, std::vector<float> *mod_rpy);
 
 }  // namespace xpr
