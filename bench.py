@@ -51,6 +51,12 @@ CONFIGS = {
                     "it=2, BF16 image/ratio storage, one batched persistent launch per phase in a CUDA graph",
                batch=64, dwidth=384, dheight=384, projections=360, sit=10, it=2, modules=3, px=0.1, rpy=2.0,
                phantom=256, ellipsoids=12, background=0.0, i0=1e5, seed=4, plain_sample=4),
+    # a request loop: Poisson arrivals of mixed-size scans, continuous batching
+    "c5": dict(desc="Poisson arrivals (4/s) of 120 scans: phantom edge in {128, 256, 384} (recon grid 1.5x: "
+                    "192 / 384 / 576), {180, 360, 720} projections on a square detector of the grid's edge, "
+                    "it 1, sit 10, 1e5 photons; FP32 and BF16 storage servers",
+               serve=True, requests=120, rate=4.0, edges=[128, 256, 384], projections_set=[180, 360, 720], sit=10,
+               it=1, px=0.1, i0=1e5, seed=5, ellipsoids=10, background=0.0),
     # one problem of the c4 family (profiling-sized)
     "c4one": dict(desc="one 384^3 recon grid of the c4 family (3 tilted modules, 36 projections per sub-iteration)",
                   batch=1, dwidth=384, dheight=384, projections=360, sit=10, it=2, modules=3, px=0.1, rpy=2.0,
@@ -696,6 +702,137 @@ def run_batched(args, cfg, rank, world, local):
     return 0
 
 
+# ----------------------------------------------------------------------------- serving (c5)
+def simulate_raw(ctx, cfg, edge, P, seed):
+    """Raw intensities (P, D, D) of a seeded ellipsoid phantom of `edge` voxels in a grid
+    of D = 1.5 edge, projected by this library's forward (FAST) with Poisson noise."""
+    import torch
+    from xpulse_recon_b200 import _lib
+    from xpulse_recon_b200.projector import geometry
+    L = _lib.lib()
+    D = int(round(1.5 * edge))
+    pd_all, g = geometry(px=cfg["px"], dwidth=D, dheight=D, projections=P, sit=1)
+    W, Hv = int(g["vwidth"]), int(g["vheight"])
+    pcfg = dict(phantom=edge, ellipsoids=cfg["ellipsoids"], background=cfg["background"])
+    phantom = make_phantom(pcfg, g["vx"], W, Hv, "cuda", seed)
+    sums = torch.zeros(P * D * D, dtype=torch.int32, device="cuda")
+    d = _lib.Launch()
+    d.vmax[:] = [W, Hv, W]
+    d.origin[:] = list(g["orig"])
+    d.voxel[:] = [g["vx"]] * 3
+    d.det_w, d.rows, d.n_angles, d.modules, d.arith = D, D, P, 1, _lib.FAST
+    dpd = torch.from_numpy(pd_all).cuda()
+    _lib.check(L.xpr_forward(ctx.handle, phantom.data_ptr(), sums.data_ptr(), dpd.data_ptr(), P, C.byref(d),
+                             C.c_void_p(torch.cuda.current_stream().cuda_stream)), "forward")
+    p = sums.to(torch.int64).bitwise_and(0xFFFFFFFF).to(torch.float32) / float(1 << 22)
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    raw = torch.poisson(cfg["i0"] * torch.exp(-p), generator=gen) / cfg["i0"]
+    out = torch.empty((P, D, D), dtype=torch.float32, pin_memory=True)  # a client's page-locked buffer
+    out.copy_(raw.view(P, D, D))
+    del sums, p, raw, phantom
+    return out.numpy(), W * Hv * W
+
+
+def run_serving(args, cfg, rank, world, local):
+    """Open loop: requests submitted at Poisson arrival times, latency percentiles from
+    the server's own clock.  Closed loop: every request submitted at once, served GUPS
+    from the makespan, against the plain FP32 path (each request alone through the
+    whole-run entry point, uploads included) on one request of each kind."""
+    import torch
+    from xpulse_recon_b200 import _lib
+    from xpulse_recon_b200.projector import Context
+    from xpulse_recon_b200.serve import DONE, Server
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    rng = np.random.default_rng(cfg["seed"])
+    kinds = [(e, P) for e in cfg["edges"] for P in cfg["projections_set"]]
+    data = {}
+    for i, (e, P) in enumerate(kinds):
+        data[(e, P)] = simulate_raw(ctx, cfg, e, P, cfg["seed"] * 100 + i)
+    torch.cuda.synchronize()
+    n = cfg["requests"]
+    reqs = []
+    for i in range(n):
+        e = cfg["edges"][rng.integers(len(cfg["edges"]))]
+        P = cfg["projections_set"][rng.integers(len(cfg["projections_set"]))]
+        params = {"recon": {"method": "naive", "it": cfg["it"], "sit": cfg["sit"], "seed": int(rng.integers(1 << 31)),
+                            "mlog": True, "weight": 1.0, "weight_factor": 0.9},
+                  "geometry": {"so": 100.0, "sd": 1000.0, "angle": 360.0}, "detector": {"px": cfg["px"]}}
+        reqs.append((params, (e, P)))
+    arrivals = np.cumsum(rng.exponential(1.0 / cfg["rate"], n))
+    # page-locked result buffers (a serving client's own); requests of one kind share one,
+    # as the benchmark reads no result
+    out_of = {k: torch.empty(data[k][1], dtype=torch.float32, pin_memory=True).numpy() for k in kinds}
+    outs = [out_of[k] for _, k in reqs]
+    pairs_of = {k: data[k][1] * k[1] for k in kinds}  # N x P per reconstruction (it 1)
+    total_pairs = sum(pairs_of[k] for _, k in reqs) * cfg["it"]
+
+    def serve(storage, open_loop):
+        srv = Server(ctx, storage=storage)
+        # warm the kernels and the allocator on one small request
+        w = srv.submit(reqs[0][0], data[reqs[0][1]][0])
+        srv.wait(w, 120.0)
+        t0 = time.perf_counter()
+        tickets = []
+        for i, (params, k) in enumerate(reqs):
+            if open_loop:
+                dt = arrivals[i] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+            tickets.append(srv.submit(params, data[k][0], outs[i]))
+        infos = [srv.wait(t, 600.0) for t in tickets]
+        ok = all(i.state == DONE for i in infos)
+        lat = np.array([i.done_s - i.submit_s for i in infos])
+        span = max(i.done_s for i in infos) - min(i.submit_s for i in infos)
+        st = srv.stats()
+        srv.close()
+        return {"ok": ok, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                "mean_s": float(lat.mean()), "gups": total_pairs / span / 1e9, "makespan_s": span,
+                "ticks": int(st.ticks), "peak_device_gb": st.peak_bytes / 1e9}
+
+    res = {}
+    serve(_lib.F32, False)  # warm-up: host threads, pools, page-locked rings
+    clocks = ClockSampler(local)
+    clocks.start()
+    for name, st in (("fp32", _lib.F32), ("bf16", _lib.BF16)):
+        res[name] = {"open_loop": serve(st, True), "saturated": serve(st, False)}
+    clk = clocks.stop()
+    # the plain FP32 path: one request of each kind alone through xpr_reconstruct_host
+    L = _lib.lib()
+    L.xpr_reconstruct_host.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.c_uint32, C.c_uint32, C.c_void_p,
+                                       C.c_uint64, C.POINTER(C.c_double)]
+    plain_pairs, plain_s = 0, 0.0
+    for k in kinds:
+        raw, N = data[k]
+        params = {"recon": {"method": "naive", "it": cfg["it"], "sit": cfg["sit"], "seed": 7, "mlog": True},
+                  "geometry": {"so": 100.0, "sd": 1000.0, "angle": 360.0}, "detector": {"px": cfg["px"]}}
+        out = np.empty(N, np.float32)
+        P, H, W = raw.shape
+        t = time.perf_counter()
+        rc = L.xpr_reconstruct_host(json.dumps(params).encode(), np.ascontiguousarray(raw).ctypes.data, P, W, H,
+                                    out.ctypes.data, out.size, C.byref(C.c_double()))
+        plain_s += time.perf_counter() - t
+        plain_pairs += pairs_of[k] * cfg["it"]
+        assert rc == 0
+    plain = plain_pairs / plain_s / 1e9
+    best = res["bf16"]["saturated"]["gups"]
+    line = {"metric": "GUPS served (voxel x projection pairs / s), with p50 / p99 request latency",
+            "value": best, "unit": "GUPS", "n_gpus": world, "steps": n, "warmup": 1,
+            "ms_per_step": 1000.0 * res["bf16"]["saturated"]["makespan_s"] / n, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 storage, f32 compute", "data": "synthetic",
+            "config": {"workload": "c5: " + cfg["desc"], "requests": n, "rate_per_s": cfg["rate"]},
+            "serving": res, "plain_fp32_e2e": {"value": plain, "unit": "GUPS",
+                                               "sample": "one request of each of the %d kinds, alone, through "
+                                                         "xpr_reconstruct_host (host images in, volume out)" % len(kinds)},
+            "speedup_vs_plain_fp32": best / plain,
+            "e2e": {"value": best, "unit": "GUPS", "h2d_bytes_per_step": int(np.mean([data[k][0].nbytes for _, k in reqs])),
+                    "d2h_bytes_per_step": int(np.mean([4 * data[k][1] for _, k in reqs]))},
+            "clocks": clk}
+    if rank == 0:
+        emit(line)
+    return 0
+
+
 def main():
     args = parse_args()
     cfg = CONFIGS[args.config]
@@ -704,6 +841,8 @@ def main():
         return run_reference(args, cfg, rank, world)
     if "batch" in cfg:
         return run_batched(args, cfg, rank, world, local)
+    if cfg.get("serve"):
+        return run_serving(args, cfg, rank, world, local)
     return run_ours(args, cfg, rank, world, local)
 
 

@@ -1,11 +1,12 @@
 // serve.cpp -- xpr_server: a request loop with continuous batching.
 //
-// Two host threads drive three CUDA streams:
+// Three host threads drive three CUDA streams:
 //   io thread       admission (first come, first served, by device-memory budget),
-//                   geometry on the host, raw projections through a pinned ring to the
-//                   device, -log / normalise into the storage type in subset-major order
-//                   (dataset.hpp:133-140), volume set to 1.0; and, at the other end,
-//                   the finished volume back to the caller and the memory freed
+//                   raw projections through a pinned ring to the device, -log /
+//                   normalise into the storage type in subset-major order
+//                   (dataset.hpp:133-140), volume set to 1.0
+//   download thread the finished volume back to the caller through a second pinned
+//                   ring, then the request's memory freed
 //   compute thread  one tick = sub-iteration k_r of every active request r as one
 //                   batched forward, error and backward launch (xpr_batch's kernels)
 // A request joins at the first tick after its upload completes and leaves after its
@@ -33,7 +34,7 @@
 namespace {
 
 constexpr uint32_t kOneBits = 0x3f800000u;  // 1.0f
-constexpr size_t kChunkBytes = 16u << 20;   // pinned upload ring: two chunks of this size (at least)
+constexpr size_t kChunkBytes = 32u << 20;   // pinned upload / download rings: two chunks of this size
 
 double now_s(std::chrono::steady_clock::time_point t0)
 {
@@ -44,6 +45,7 @@ struct Request {
     uint64_t ticket = 0;
     xpr::Params p;
     const float *raw = nullptr;
+    bool raw_pinned = false, out_pinned = false;  // page-locked caller buffers: copied without staging
     int64_t P = 0;
     uint32_t W = 0, H = 0;
     float *out = nullptr;
@@ -75,7 +77,7 @@ struct xpr_server {
     std::chrono::steady_clock::time_point t0;
     // state
     std::mutex mu;
-    std::condition_variable cv_io, cv_compute, cv_done;
+    std::condition_variable cv_io, cv_compute, cv_done, cv_dl;
     bool stop = false;
     uint64_t next_ticket = 1;
     std::map<uint64_t, std::unique_ptr<Request>> reqs;
@@ -84,8 +86,11 @@ struct xpr_server {
     uint64_t bytes_in_use = 0, peak_bytes = 0;
     xpr_serve_stats stats{};
     // io resources
-    cudaStream_t io = nullptr, comp = nullptr;
+    cudaStream_t io = nullptr, comp = nullptr, dl = nullptr;
     void *pinned[2] = {nullptr, nullptr};
+    void *dl_pinned[2] = {nullptr, nullptr};  // download ring of dl_bytes per chunk
+    size_t dl_bytes = 0;
+    cudaEvent_t dl_ev[2] = {nullptr, nullptr};
     float *dstage[2] = {nullptr, nullptr};
     cudaEvent_t chunk_ev[2] = {nullptr, nullptr};
     size_t chunk_bytes = 0;
@@ -97,12 +102,25 @@ struct xpr_server {
     size_t items_cap = 0;
     cudaEvent_t tick_ev[2] = {nullptr, nullptr};
     unsigned grid_fwd = 0, grid_bwd = 0;
-    std::thread io_thread, compute_thread;
+    std::thread io_thread, compute_thread, dl_thread;
 };
 
 namespace {
 
 int fail(int code, const char *msg) { return xpr::set_last_error(code, "%s", msg); }
+
+// host copy to or from pinned staging, split over a few host threads (one thread
+// copies at well under the host memory bandwidth)
+void par_memcpy(void *dst, const void *src, size_t n)
+{
+    constexpr size_t kTask = 4u << 20;
+    const int64_t tasks = (int64_t)((n + kTask - 1) / kTask);
+#pragma omp parallel for schedule(static) num_threads(8) if (tasks > 1)
+    for (int64_t t = 0; t < tasks; ++t) {
+        const size_t o = (size_t)t * kTask;
+        std::memcpy((char *)dst + o, (const char *)src + o, std::min(kTask, n - o));
+    }
+}
 
 void check_cuda(cudaError_t e, const char *what)
 {
@@ -125,6 +143,11 @@ bool ensure_chunks(xpr_server *s, size_t bytes)
         if (cudaHostAlloc(&s->pinned[b], bytes, cudaHostAllocDefault) != cudaSuccess) return false;
         if (cudaMalloc((void **)&s->dstage[b], bytes) != cudaSuccess) return false;
     }
+    // the download ring keeps the size it was made with (the download thread owns it)
+    for (int b = 0; b < 2 && !s->dl_pinned[b]; ++b) {
+        if (cudaHostAlloc(&s->dl_pinned[b], bytes, cudaHostAllocDefault) != cudaSuccess) return false;
+        s->dl_bytes = bytes;
+    }
     s->chunk_bytes = bytes;
     return true;
 }
@@ -142,9 +165,12 @@ void stream_images(xpr_server *s, Request *r, int64_t n_img, F &&per_chunk)
     for (int64_t i0 = 0; i0 < n_img; i0 += per, b ^= 1) {
         const int64_t n = std::min(per, n_img - i0);
         check_cuda(cudaEventSynchronize(s->chunk_ev[b]), "staging");
-        std::memcpy(s->pinned[b], r->raw + (size_t)i0 * r->W * r->H, (size_t)n * img_bytes);
-        check_cuda(cudaMemcpyAsync(s->dstage[b], s->pinned[b], (size_t)n * img_bytes, cudaMemcpyHostToDevice, s->io),
-                   "upload");
+        const float *src = r->raw + (size_t)i0 * r->W * r->H;
+        if (!r->raw_pinned) {
+            par_memcpy(s->pinned[b], src, (size_t)n * img_bytes);
+            src = (const float *)s->pinned[b];
+        }
+        check_cuda(cudaMemcpyAsync(s->dstage[b], src, (size_t)n * img_bytes, cudaMemcpyHostToDevice, s->io), "upload");
         per_chunk(i0, n, s->dstage[b]);
         check_cuda(cudaEventRecord(s->chunk_ev[b], s->io), "staging");
     }
@@ -209,15 +235,44 @@ void upload_request(xpr_server *s, Request *r)
     check_cuda(cudaEventRecord(r->ready, s->io), "event");
 }
 
+// The finished volume back to the caller through the download ring (device -> pinned
+// on the download stream, pinned -> caller by host threads, the two overlapped), then
+// its memory freed.
 void finish_request(xpr_server *s, Request *r)
 {
     int err = r->error;  // set by the compute thread when a tick failed
     cudaError_t e = cudaEventSynchronize(r->done_ev);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(r->out, r->pp.p.vol, 4 * r->N, cudaMemcpyDeviceToHost, s->io);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->io);
-    if (e != cudaSuccess) err = XPR_ERR_CUDA;
-    if (r->arena) cudaFreeAsync(r->arena, s->io);
+    const size_t total = 4 * r->N;
+    const char *src = (const char *)r->pp.p.vol;
+    char *dst = (char *)r->out;
+    size_t pending[2] = {0, 0}, pending_off[2] = {0, 0};
+    int b = 0;
+    if (r->out_pinned && e == cudaSuccess) {  // straight into the caller's page-locked buffer
+        e = cudaMemcpyAsync(dst, src, total, cudaMemcpyDeviceToHost, s->dl);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->dl);
+    }
+    for (size_t off = 0; !r->out_pinned && e == cudaSuccess && off < total; off += s->dl_bytes, b ^= 1) {
+        const size_t n = std::min(s->dl_bytes, total - off);
+        if (pending[b]) {  // drain the chunk that used this buffer two copies ago
+            e = cudaEventSynchronize(s->dl_ev[b]);
+            if (e == cudaSuccess) par_memcpy(dst + pending_off[b], s->dl_pinned[b], pending[b]);
+            pending[b] = 0;
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s->dl_pinned[b], src + off, n, cudaMemcpyDeviceToHost, s->dl);
+        if (e == cudaSuccess) e = cudaEventRecord(s->dl_ev[b], s->dl);
+        pending[b] = n;
+        pending_off[b] = off;
+    }
+    for (int k = 0; k < 2; ++k) {
+        b ^= 1;
+        if (e == cudaSuccess && pending[b]) {
+            e = cudaEventSynchronize(s->dl_ev[b]);
+            if (e == cudaSuccess) par_memcpy(dst + pending_off[b], s->dl_pinned[b], pending[b]);
+        }
+        pending[b] = 0;
+    }
+    if (e != cudaSuccess && !err) err = XPR_ERR_CUDA;
+    if (r->arena) cudaFreeAsync(r->arena, s->dl);
     r->arena = nullptr;
     std::lock_guard<std::mutex> lk(s->mu);
     s->bytes_in_use -= r->bytes;
@@ -227,14 +282,15 @@ void finish_request(xpr_server *s, Request *r)
     if (err) ++s->stats.failed;
     else ++s->stats.completed;
     s->cv_done.notify_all();
+    s->cv_io.notify_all();  // memory freed: admission may proceed
 }
 
-void io_loop(xpr_server *s)
+void dl_loop(xpr_server *s)
 {
     xpr::context_device(s->ctx);
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
-        if (!s->finishing.empty()) {  // completions first: they free memory
+        if (!s->finishing.empty()) {
             Request *r = s->finishing.front();
             s->finishing.pop_front();
             lk.unlock();
@@ -242,6 +298,16 @@ void io_loop(xpr_server *s)
             lk.lock();
             continue;
         }
+        if (s->stop && s->queue.empty() && s->ready.empty() && s->active.empty()) break;
+        s->cv_dl.wait(lk);
+    }
+}
+
+void io_loop(xpr_server *s)
+{
+    xpr::context_device(s->ctx);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
         if (!s->queue.empty()) {
             Request *r = s->queue.front();
             const uint64_t resident = s->active.size() + s->ready.size();
@@ -276,7 +342,7 @@ void io_loop(xpr_server *s)
                 continue;
             }
         }
-        if (s->stop && s->queue.empty() && s->ready.empty() && s->active.empty() && s->finishing.empty()) break;
+        if (s->stop && s->queue.empty()) break;
         s->cv_io.wait(lk);
     }
 }
@@ -378,9 +444,9 @@ void compute_loop(xpr_server *s)
             }
         }
         s->active = left;  // only this thread changes s->active
-        if (!s->finishing.empty()) s->cv_io.notify_all();
+        if (!s->finishing.empty()) s->cv_dl.notify_all();
     }
-    s->cv_io.notify_all();
+    s->cv_dl.notify_all();
 }
 
 // ------------------------------------------------------------------------ submission
@@ -437,6 +503,8 @@ void release(xpr_server *s)
         if (s->items_host[b]) cudaFreeHost(s->items_host[b]);
         if (s->items_dev[b]) cudaFree(s->items_dev[b]);
         if (s->tick_ev[b]) cudaEventDestroy(s->tick_ev[b]);
+        if (s->dl_pinned[b]) cudaFreeHost(s->dl_pinned[b]);
+        if (s->dl_ev[b]) cudaEventDestroy(s->dl_ev[b]);
     }
     for (auto &kv : s->reqs) {
         if (kv.second->ready) cudaEventDestroy(kv.second->ready);
@@ -446,6 +514,7 @@ void release(xpr_server *s)
     if (s->minmax) cudaFree(s->minmax);
     if (s->io) cudaStreamDestroy(s->io);
     if (s->comp) cudaStreamDestroy(s->comp);
+    if (s->dl) cudaStreamDestroy(s->dl);
     delete s;
 }
 
@@ -489,8 +558,10 @@ int xpr_serve_create(xpr_ctx *ctx, const xpr_serve_opts *opts, xpr_server **out)
     s->opts = o;
     cudaError_t e = cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->comp, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->dl, cudaStreamNonBlocking);
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
-        if ((e = cudaEventCreateWithFlags(&s->chunk_ev[b], cudaEventDisableTiming)) == cudaSuccess)
+        if ((e = cudaEventCreateWithFlags(&s->chunk_ev[b], cudaEventDisableTiming)) == cudaSuccess &&
+            (e = cudaEventCreateWithFlags(&s->dl_ev[b], cudaEventDisableTiming)) == cudaSuccess)
             e = cudaEventCreateWithFlags(&s->tick_ev[b], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaMalloc((void **)&s->tickets, 256);
@@ -504,6 +575,7 @@ int xpr_serve_create(xpr_ctx *ctx, const xpr_serve_opts *opts, xpr_server **out)
     s->grid_bwd = (unsigned)(di->sm_count * std::max(1, xpr::batched_ctas_per_sm(1, o.arith, o.storage, 16)));
     s->io_thread = std::thread(io_loop, s);
     s->compute_thread = std::thread(compute_loop, s);
+    s->dl_thread = std::thread(dl_loop, s);
     *out = s;
     return XPR_OK;
 }
@@ -529,6 +601,16 @@ int xpr_serve_submit(xpr_server *s, const char *json, const float *raw, int64_t 
                                                 "is %llu", (unsigned long long)r->bytes,
                                    (unsigned long long)s->opts.mem_budget);
     if (!xpr::context_device(s->ctx)) return XPR_ERR_INVALID;
+    auto pinned = [](const void *p) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
+    };
+    r->raw_pinned = pinned(raw) && pinned(raw + (size_t)count * width * height - 1);
+    r->out_pinned = pinned(vol_out) && pinned(vol_out + r->N - 1);
     if (cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&r->done_ev, cudaEventDisableTiming) != cudaSuccess)
         return fail(XPR_ERR_CUDA, "xpr_serve_submit: events");
@@ -589,15 +671,18 @@ int xpr_serve_destroy(xpr_server *s)
         s->cv_io.notify_all();
         s->cv_compute.notify_all();
     }
-    s->compute_thread.join();
+    s->compute_thread.join();  // returns once nothing is queued, uploading or active
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->cv_io.notify_all();
+        s->cv_dl.notify_all();
     }
     s->io_thread.join();
+    s->dl_thread.join();
     xpr::context_device(s->ctx);
     cudaStreamSynchronize(s->io);
     cudaStreamSynchronize(s->comp);
+    cudaStreamSynchronize(s->dl);
     release(s);
     return XPR_OK;
 }

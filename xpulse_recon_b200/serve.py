@@ -77,12 +77,16 @@ class Server:
         self.handle = h
         self._keep = {}
 
-    def submit(self, params: dict, raw: np.ndarray) -> int:
-        """raw: (projections, height, width) float32 intensities.  Returns the ticket."""
+    def submit(self, params: dict, raw: np.ndarray, out: np.ndarray = None) -> int:
+        """raw: (projections, height, width) float32 intensities; out: optional float32
+        array of the grid's size for the result (page-locked buffers -- e.g. numpy views
+        of pinned torch tensors -- are copied without staging).  Returns the ticket."""
         raw = np.ascontiguousarray(raw, np.float32)
         P, H, W = raw.shape
         vw, vh = grid_of(params, W, H)
-        out = np.full(vw * vh * vw, np.nan, np.float32)
+        if out is None:
+            out = np.full(vw * vh * vw, np.nan, np.float32)
+        assert out.dtype == np.float32 and out.flags.c_contiguous and out.size >= vw * vh * vw
         t = C.c_uint64()
         check(lib().xpr_serve_submit(self.handle, json.dumps(params).encode(), raw.ctypes.data, P, W, H,
                                      out.ctypes.data, out.size, C.byref(t)), "xpr_serve_submit")
