@@ -82,6 +82,9 @@ def parse_args():
                    help="image / ratio storage (default: fp32; bf16 for the batched configurations)")
     p.add_argument("--config", choices=sorted(CONFIGS), default="c2")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--shard", action="store_true",
+                   help="N > 1: one reconstruction split into y-slabs over the ranks (u32 all-reduce of the "
+                        "detector sums per sub-iteration, strong scaling) instead of one per rank")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     return p.parse_args()
 
@@ -833,6 +836,66 @@ def run_serving(args, cfg, rank, world, local):
     return 0
 
 
+# ----------------------------------------------------------------------------- slab-sharded
+def run_sharded(args, cfg, rank, world, local):
+    """One c2 reconstruction split into y-slabs over the ranks (xpulse_recon_b200.shard):
+    per sub-iteration a slab forward, an NCCL all-reduce of the u32 detector sums, the
+    error and a slab backward.  Total work is fixed as N grows (strong scaling)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from xpulse_recon_b200.shard import GpuOps, SlabReconstruction
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    args.storage = args.storage or "fp32"
+    prob = Problem(cfg, args.arith, args.storage, local, cfg["seed"])  # the same measured data on every rank
+    images = torch.cat(prob.images)
+    del prob.vol, prob.sums, prob.ratio, prob.phantom
+    torch.cuda.empty_cache()
+    K, Wm = args.steps, args.warmup
+    steps = Wm + K + 1
+    ops = GpuOps(prob.ctx, prob.arith, prob.storage)
+    r = SlabReconstruction(ops, None, prob.pd_all, prob.g, it=-(-steps // prob.S), sit=prob.S, seed=cfg["seed"],
+                           rank=rank, world=world, images=images, shape=(prob.P, prob.Hd, prob.Wd))
+    for k in range(Wm + 1):  # step 0 has no forward: warm-up starts with it
+        r.step(k)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0.record()
+    for k in range(Wm + 1, Wm + 1 + K):
+        r.step(k)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    pairs_step = prob.W * prob.Hv * prob.W * prob.Pc
+    value = pairs_step * K / (ms / 1000.0) / 1e9
+    line = {"metric": "GUPS per sub-iteration (voxel x projection pairs / s)", "value": value, "unit": "GUPS",
+            "n_gpus": world, "steps": K, "warmup": Wm + 1, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config + ": " + cfg["desc"], "parallelism": "y-slab sharding, %d ranks, "
+                       "u32 all-reduce of the detector sums" % world, "arith": args.arith, "storage": args.storage,
+                       "l2": "inputs larger than L2"},
+            "exchange_bytes_per_step": 4 * prob.npix if world > 1 else 0, "gpu_launches": 3 * K,
+            "clocks": clk}
+    if rank == 0:
+        emit(line)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse_args()
     cfg = CONFIGS[args.config]
@@ -843,6 +906,8 @@ def main():
         return run_batched(args, cfg, rank, world, local)
     if cfg.get("serve"):
         return run_serving(args, cfg, rank, world, local)
+    if args.shard:
+        return run_sharded(args, cfg, rank, world, local)
     return run_ours(args, cfg, rank, world, local)
 
 
