@@ -57,6 +57,13 @@ CONFIGS = {
                     "it 1, sit 10, 1e5 photons; FP32 and BF16 storage servers",
                serve=True, requests=120, rate=4.0, edges=[128, 256, 384], projections_set=[180, 360, 720], sit=10,
                it=1, px=0.1, i0=1e5, seed=5, ellipsoids=10, background=0.0),
+    # out-of-core at half linear scale: the volume does not fit the device-memory cap
+    "c3h": dict(desc="c3 at half linear scale: 1536x1024x1536 recon grid (9.7 GB), 1000 projections of "
+                     "1536x1024 (6.3 GB), sit 20 -> 50, it 1, under an 8 GB device-memory cap: naive without "
+                     "the cap, then method_1b, method_1c and method_2 with it",
+                outofcore=True, dwidth=1536, dheight=1024, projections=1000, sit=20, it=1, px=0.1, so=100.0,
+                sd=1000.0, phantom=1024, ellipsoids=60, background=0.0, i0=5e4, seed=3, mem_cap=8 << 30,
+                methods=["naive", "method_1b", "method_1c", "method_2"]),
     # one problem of the c4 family (profiling-sized)
     "c4one": dict(desc="one 384^3 recon grid of the c4 family (3 tilted modules, 36 projections per sub-iteration)",
                   batch=1, dwidth=384, dheight=384, projections=360, sit=10, it=2, modules=3, px=0.1, rpy=2.0,
@@ -896,6 +903,93 @@ def run_sharded(args, cfg, rank, world, local):
     return 0
 
 
+# ----------------------------------------------------------------------------- out-of-core (c3)
+def host_available_bytes():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def run_outofcore(args, cfg, rank, world, local):
+    """Whole reconstructions through the drop-in entry point (xpr_reconstruct_host: host
+    projections in, host volume out) with each memory mode; the streaming modes under a
+    device-memory cap smaller than the volume."""
+    import torch
+    from xpulse_recon_b200 import _lib
+    from xpulse_recon_b200.projector import Context, geometry
+    P, Wd, Hd = cfg["projections"], cfg["dwidth"], cfg["dheight"]
+    # host memory: projections and volume here, and the streaming modes' pinned copies of both
+    need = 2 * (4 * P * Wd * Hd) + 2 * (4 * Wd * Hd * Wd)
+    avail = host_available_bytes()
+    if avail and need > avail // 2:
+        emit({"metric": "GUPS per sub-iteration (voxel x projection pairs / s)", "value": None,
+              "unavailable": "needs %.1f GB of host memory, %.1f GB available" % (need / 1e9, avail / 1e9)})
+        return 0
+    torch.cuda.set_device(local)
+    L = _lib.lib()
+    ctx = Context(local)
+    pd_all, g = geometry(so=cfg["so"], sd=cfg["sd"], px=cfg["px"], dwidth=Wd, dheight=Hd, projections=P, sit=1)
+    W, Hv = int(g["vwidth"]), int(g["vheight"])
+    N = W * Hv * W
+    phantom = make_phantom(cfg, g["vx"], W, Hv, "cuda", cfg["seed"])
+    raw = np.empty((P, Hd, Wd), np.float32)
+    gen = torch.Generator(device="cuda").manual_seed(cfg["seed"])
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    chunk = 50
+    for a in range(0, P, chunk):  # simulate a chunk of projections at a time (bounded device memory)
+        n = min(chunk, P - a)
+        sums = torch.zeros(n * Wd * Hd, dtype=torch.int32, device="cuda")
+        d = _lib.Launch()
+        d.vmax[:] = [W, Hv, W]
+        d.origin[:] = list(g["orig"])
+        d.voxel[:] = [g["vx"]] * 3
+        d.det_w, d.rows, d.n_angles, d.modules, d.arith = Wd, Hd, n, 1, _lib.FAST
+        dpd = torch.from_numpy(np.ascontiguousarray(pd_all[a:a + n])).cuda()
+        _lib.check(L.xpr_forward(ctx.handle, phantom.data_ptr(), sums.data_ptr(), dpd.data_ptr(), n, C.byref(d), sp),
+                   "forward")
+        p = sums.to(torch.int64).bitwise_and(0xFFFFFFFF).to(torch.float32) / float(1 << 22)
+        raw[a:a + n] = (torch.poisson(cfg["i0"] * torch.exp(-p), generator=gen) / cfg["i0"]).view(n, Hd, Wd).cpu()
+        del sums, p
+    del phantom
+    torch.cuda.empty_cache()
+    ctx.close()
+    L.xpr_reconstruct_host.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.c_uint32, C.c_uint32, C.c_void_p,
+                                       C.c_uint64, C.POINTER(C.c_double)]
+    out = np.empty(N, np.float32)
+    results = {}
+    pairs = N * (P // cfg["sit"]) * cfg["sit"] * cfg["it"]
+    clocks = ClockSampler(local)
+    clocks.start()
+    for m in cfg["methods"]:
+        params = {"recon": {"method": m, "it": cfg["it"], "sit": cfg["sit"], "seed": 11, "mlog": True,
+                            "mem_cap": 0 if m == "naive" else cfg["mem_cap"]},
+                  "geometry": {"so": cfg["so"], "sd": cfg["sd"], "angle": 360.0}, "detector": {"px": cfg["px"]}}
+        secs = C.c_double()
+        t = time.perf_counter()
+        rc = L.xpr_reconstruct_host(json.dumps(params).encode(), raw.ctypes.data, P, Wd, Hd, out.ctypes.data, N,
+                                    C.byref(secs))
+        wall = time.perf_counter() - t
+        results[m] = {"rc": rc, "iterations_s": secs.value, "wall_s": wall,
+                      "gups_iterations": pairs / max(secs.value, 1e-9) / 1e9, "gups_e2e": pairs / wall / 1e9,
+                      "finite": float(np.isfinite(out).mean())}
+    clk = clocks.stop()
+    best = max(results[m]["gups_e2e"] for m in cfg["methods"] if m != "naive")
+    line = {"metric": "GUPS per sub-iteration (voxel x projection pairs / s)", "value": best, "unit": "GUPS",
+            "n_gpus": 1, "steps": cfg["sit"] * cfg["it"], "warmup": 0, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "c3h: " + cfg["desc"], "grid": [W, Hv, W], "mem_cap_bytes": cfg["mem_cap"]},
+            "methods": results, "clocks": clk,
+            "e2e": {"value": best, "unit": "GUPS", "h2d_bytes_per_step": int(raw.nbytes // cfg["sit"]),
+                    "d2h_bytes_per_step": int(4 * N // cfg["sit"])}}
+    emit(line)
+    return 0
+
+
 def main():
     args = parse_args()
     cfg = CONFIGS[args.config]
@@ -908,6 +1002,8 @@ def main():
         return run_serving(args, cfg, rank, world, local)
     if args.shard:
         return run_sharded(args, cfg, rank, world, local)
+    if cfg.get("outofcore"):
+        return run_outofcore(args, cfg, rank, world, local)
     return run_ours(args, cfg, rank, world, local)
 
 
