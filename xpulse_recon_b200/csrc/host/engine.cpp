@@ -1,5 +1,6 @@
 // engine.cpp -- see engine.h
 #include "engine.h"
+#include "hostcopy.h"
 
 #include <cuda_runtime.h>
 
@@ -142,7 +143,7 @@ public:
     int64_t count() const override { return n_; }
     uint32_t width() const override { return w_; }
     uint32_t height() const override { return h_; }
-    void read(int64_t i, float *dst) override { std::memcpy(dst, d_ + (size_t)i * w_ * h_, sizeof(float) * w_ * h_); }
+    void read(int64_t i, float *dst) override { par_memcpy(dst, d_ + (size_t)i * w_ * h_, sizeof(float) * w_ * h_); }
 
 private:
     const float *d_;
@@ -217,18 +218,33 @@ struct Engine::Impl {
 
     // Reads every image, preprocesses it on the device (data_loader.hpp:48-101) and hands the
     // preprocessed image (storage dtype, device) to sink(i, ptr) on the compute stream.
+    // The images one by one through two page-locked staging buffers: reading image i + 1
+    // on the host overlaps the upload and preprocessing of image i on the stream; `sink`
+    // enqueues its copy of the preprocessed image on the same stream.
     void preprocess(const Params &p, const std::function<void(int64_t, const void *)> &sink)
     {
-        DevBuf raw(ctx, WH * 4), out(ctx, WH * esize), mm(ctx, 8);
-        PinBuf stage(ctx, WH * 4);
+        DevBuf raw[2] = {DevBuf(ctx, WH * 4), DevBuf(ctx, WH * 4)};
+        DevBuf out[2] = {DevBuf(ctx, WH * esize), DevBuf(ctx, WH * esize)};
+        DevBuf mm(ctx, 8);
+        PinBuf stage0(ctx, WH * 4), stage1(ctx, WH * 4);
+        PinBuf *stage[2] = {&stage0, &stage1};
+        Event used[2];
+        bool pending[2] = {false, false};
+        auto next = [&](int64_t i) {  // image i into staging buffer i % 2, uploaded to raw[i % 2]
+            const int b = (int)(i & 1);
+            if (pending[b]) check_cuda(cudaEventSynchronize(used[b].e), "staging");
+            src->read(i, stage[b]->as<float>());
+            check(xpr_upload(ctx, raw[b].p, stage[b]->p, WH * 4, comp->v()), "upload");
+            return b;
+        };
         const float init[2] = {FLT_MAX, FLT_MIN};  // data_loader.hpp:12-13
         if (p.normalize) {
             check(xpr_upload(ctx, mm.p, init, 8, comp->v()), "upload");
             for (int64_t i = 0; i < P; ++i) {
-                comp->sync();
-                src->read(i, stage.as<float>());
-                check(xpr_upload(ctx, raw.p, stage.p, WH * 4, comp->v()), "upload");
-                check(xpr_preprocess_minmax(ctx, raw.as<float>(), WH, mm.as<float>(), comp->v()), "minmax");
+                const int b = next(i);
+                check(xpr_preprocess_minmax(ctx, raw[b].as<float>(), WH, mm.as<float>(), comp->v()), "minmax");
+                used[b].record(*comp);
+                pending[b] = true;
             }
             float h[2];
             check(xpr_download(ctx, h, mm.p, 8, comp->v()), "download");
@@ -237,14 +253,50 @@ struct Engine::Impl {
             nmax = h[1];
         }
         for (int64_t i = 0; i < P; ++i) {
-            comp->sync();
-            src->read(i, stage.as<float>());
-            check(xpr_upload(ctx, raw.p, stage.p, WH * 4, comp->v()), "upload");
-            check(xpr_preprocess_apply(ctx, raw.as<float>(), out.p, dtype, WH, p.normalize ? 1 : 0, mm.as<float>(),
-                                       p.mlog ? 1 : 0, comp->v()), "preprocess");
-            sink(i, out.p);
+            const int b = next(i);
+            check(xpr_preprocess_apply(ctx, raw[b].as<float>(), out[b].p, dtype, WH, p.normalize ? 1 : 0,
+                                       mm.as<float>(), p.mlog ? 1 : 0, comp->v()), "preprocess");
+            sink(i, out[b].p);
+            used[b].record(*comp);
+            pending[b] = true;
         }
         comp->sync();
+    }
+
+    // n bytes of device memory to host memory: straight into page-locked memory, otherwise
+    // through two page-locked chunks whose host copies overlap the next chunk's transfer
+    void download_host(void *dst, const void *dsrc, uint64_t n)
+    {
+        cudaPointerAttributes at{};
+        const bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (pinned || n <= (8u << 20)) {
+            check(xpr_download(ctx, dst, dsrc, n, comp->v()), "download");
+            comp->sync();
+            return;
+        }
+        const uint64_t chunk = 64u << 20;
+        PinBuf c0(ctx, chunk), c1(ctx, chunk);
+        PinBuf *cb[2] = {&c0, &c1};
+        Event done[2];
+        uint64_t pend[2] = {0, 0}, pend_off[2] = {0, 0};
+        int b = 0;
+        for (uint64_t off = 0; off < n; off += chunk, b ^= 1) {
+            if (pend[b]) {
+                check_cuda(cudaEventSynchronize(done[b].e), "download");
+                par_memcpy((char *)dst + pend_off[b], cb[b]->p, pend[b]);
+            }
+            const uint64_t m = std::min(chunk, n - off);
+            check(xpr_download(ctx, cb[b]->p, (const char *)dsrc + off, m, comp->v()), "download");
+            done[b].record(*comp);
+            pend[b] = m;
+            pend_off[b] = off;
+        }
+        for (int k = 0; k < 2; ++k, b ^= 1) {
+            if (!pend[b]) continue;
+            check_cuda(cudaEventSynchronize(done[b].e), "download");
+            par_memcpy((char *)dst + pend_off[b], cb[b]->p, pend[b]);
+        }
     }
 
     xpr_launch launch(int32_t y0, int32_t y1, const float origin[3], float vx, uint32_t rows, int32_t row_offset,
@@ -340,7 +392,12 @@ void Engine::reconstruct()
     const int64_t W = d.W, Hv = d.Hv, S = d.S, Pc = d.Pc, M = d.M;
     const size_t PDB = sizeof(xpr_projdata);
     float origin[3];
-    volume_.assign(N, NAN);
+    // the result goes to the caller's buffer when one is set, else to volume_
+    float *vout = out_;
+    if (!vout) {
+        volume_.resize(N);
+        vout = volume_.data();
+    }
 
     if (p.method == Method::naive) {
         const uint64_t nvol = p.compat_pad ? xpr_ndrange(N) : N;
@@ -386,11 +443,10 @@ void Engine::reconstruct()
         d.comp->sync();
         stats_.seconds_iterations = now() - t1;
         std::cout << "Ok" << std::endl;
-        check(xpr_download(d.ctx, volume_.data(), vol.p, N * 4, d.comp->v()), "download");
-        d.comp->sync();
+        d.download_host(vout, vol.p, N * 4);
         if (d.write) {
             std::cout << "Saving result..." << std::flush;
-            d.save_layers(p, volume_.data(), 0, Hv);
+            d.save_layers(p, vout, 0, Hv);
             std::cout << "Ok" << std::endl;
         }
         stats_.seconds_total = now() - t0;
@@ -544,8 +600,8 @@ void Engine::reconstruct()
         }
         stats_.seconds_iterations = now() - t1;
         std::cout << "Ok" << std::endl;
-        std::memcpy(volume_.data(), hvol.p, N * 4);
-        if (d.write) d.save_layers(p, volume_.data(), 0, Hv);
+        par_memcpy(vout, hvol.p, N * 4);
+        if (d.write) d.save_layers(p, vout, 0, Hv);
         stats_.seconds_total = now() - t0;
         return;
     }
@@ -560,6 +616,15 @@ void Engine::reconstruct()
         std::cout << "Chunks : ";
         for (const auto &c : chunks) std::cout << " [" << c.vOffset << "-" << c.vOffset + c.vSize << "],";
         std::cout << std::endl;
+        // layers no chunk reconstructs are NaN
+        {
+            std::vector<char> covered((size_t)Hv, 0);
+            for (const auto &c : chunks)
+                for (int64_t l = c.vOffset; l < c.vOffset + c.vSize && l < Hv; ++l)
+                    if (l >= 0 && c.vSize > 0 && c.iSize > 0) covered[(size_t)l] = 1;
+            for (int64_t l = 0; l < Hv; ++l)
+                if (!covered[(size_t)l]) std::fill(vout + (uint64_t)l * W * W, vout + (uint64_t)(l + 1) * W * W, NAN);
+        }
         const bool sep = d.dtype != XPR_F32;
         PinBuf himg(d.ctx, (uint64_t)(S * Pc) * WH * d.esize);
         std::cout << "Pre-processing images..." << std::flush;
@@ -605,10 +670,9 @@ void Engine::reconstruct()
                 }
                 weight *= p.weight_factor;
             }
-            check(xpr_download(d.ctx, volume_.data() + (uint64_t)c.vOffset * W * W, slab.at((uint64_t)c.vPadTop * W * W * 4),
-                               (uint64_t)c.vSize * W * W * 4, d.comp->v()), "download");
-            d.comp->sync();
-            if (d.write) d.save_layers(p, volume_.data() + (uint64_t)c.vOffset * W * W, c.vOffset, c.vOffset + c.vSize);
+            d.download_host(vout + (uint64_t)c.vOffset * W * W, slab.at((uint64_t)c.vPadTop * W * W * 4),
+                            (uint64_t)c.vSize * W * W * 4);
+            if (d.write) d.save_layers(p, vout + (uint64_t)c.vOffset * W * W, c.vOffset, c.vOffset + c.vSize);
             std::cout << "Done." << std::endl;
         }
         stats_.seconds_iterations = now() - t1;

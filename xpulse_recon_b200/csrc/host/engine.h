@@ -53,6 +53,8 @@ public:
     Engine(const Engine &) = delete;
     Engine &operator=(const Engine &) = delete;
 
+    // Results into `dst` (vwidth * vheight * vwidth floats, the caller's) instead of volume().
+    void set_output(float *dst) { out_ = dst; }
     void reconstruct();       // exec() of the selected method
     void simulate();          // forward_exec() of the volume in the output directory
     const std::vector<float> &volume() const { return volume_; }
@@ -67,6 +69,7 @@ private:
     xpr_geom_params gp_{};
     xpr_geom_out go_{};
     std::vector<float> volume_;
+    float *out_ = nullptr;
     RunStats stats_;
 };
 

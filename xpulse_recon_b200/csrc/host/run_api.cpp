@@ -70,10 +70,10 @@ int xpr_reconstruct_host(const char *json, const float *images, int64_t count, u
     try {
         xpr::Params p = xpr::load_params(json ? json : "{}");
         xpr::Engine eng(p, xpr::memory_images(images, count, width, height), false);
+        const uint64_t n = (uint64_t)eng.vwidth() * eng.vheight() * eng.vwidth();
+        if (n > vol_cap) return XPR_ERR_INVALID;
+        eng.set_output(vol_out);  // straight into the caller's buffer
         eng.reconstruct();
-        const auto &v = eng.volume();
-        if (v.size() > vol_cap) return XPR_ERR_INVALID;
-        std::memcpy(vol_out, v.data(), v.size() * sizeof(float));
         if (seconds) *seconds = eng.stats().seconds_iterations;
         return XPR_OK;
     } catch (const std::exception &e) {

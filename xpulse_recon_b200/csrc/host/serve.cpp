@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "batch_plan.h"
+#include "hostcopy.h"
 #include "params.h"
 
 namespace {
@@ -109,18 +110,7 @@ namespace {
 
 int fail(int code, const char *msg) { return xpr::set_last_error(code, "%s", msg); }
 
-// host copy to or from pinned staging, split over a few host threads (one thread
-// copies at well under the host memory bandwidth)
-void par_memcpy(void *dst, const void *src, size_t n)
-{
-    constexpr size_t kTask = 4u << 20;
-    const int64_t tasks = (int64_t)((n + kTask - 1) / kTask);
-#pragma omp parallel for schedule(static) num_threads(8) if (tasks > 1)
-    for (int64_t t = 0; t < tasks; ++t) {
-        const size_t o = (size_t)t * kTask;
-        std::memcpy((char *)dst + o, (const char *)src + o, std::min(kTask, n - o));
-    }
-}
+using xpr::par_memcpy;
 
 void check_cuda(cudaError_t e, const char *what)
 {
