@@ -497,106 +497,195 @@ void Engine::reconstruct()
                                        cudaMemcpyDeviceToHost, d.comp->s), "copy");
         });
         std::cout << "Ok." << std::endl;
-        // slab size: what fits next to the images (double-buffered unless method_1a)
         const uint64_t layer_bytes = (uint64_t)W * W * 4;
-        const uint64_t avail = d.available();
-        const int nbuf = sync_mode ? 1 : 2;
-        const uint64_t budget = avail > (64ull << 20) ? (avail - (64ull << 20)) / nbuf : layer_bytes;
-        int64_t slab = std::max<int64_t>(1, std::min<int64_t>(Hv, (int64_t)(budget / layer_bytes)));
-        if (p.slab > 0) slab = std::min<int64_t>(slab, p.slab);
-        std::vector<DevBuf> sb;
-        for (int b = 0; b < nbuf; ++b) sb.emplace_back(d.ctx, (uint64_t)slab * layer_bytes);
         const float init = lplh ? 1.0f / (float)std::sqrt((double)(W * W)) : 1.0f;  // reconstruction_lplh.hpp:194
-        for (uint64_t i = 0; i < N; ++i) hvol.as<float>()[i] = init;
+        float *hv = hvol.as<float>();
+#pragma omp parallel for schedule(static) num_threads(8)
+        for (int64_t i = 0; i < (int64_t)N; ++i) hv[i] = init;
         if (!lplh)  // reconstruction_lpla.hpp:243
             check(xpr_fill_u32(d.ctx, sum.p, 1u << 22, (uint64_t)slots * WH, d.comp->v()), "fill");
-        Event e_up[2], e_done[2], e_free[2], e_img;
-        std::cout << "Executing reconstruction..." << std::flush;
-        const double t1 = now();
-        float weight = p.weight;
-        const int64_t nslab = (Hv + slab - 1) / slab;
-        for (int64_t mit = 0; mit < p.it; ++mit) {
-            for (int64_t sit = 0; sit < S; ++sit) {
-                d.jittered_origin(go_, origin);
-                const bool first = (mit == 0 && sit == 0);
-                const int64_t nimg = lplh ? d.angles_in(sit) : Pc;
-                check(xpr_upload(d.ctx, img.p, himg.at((uint64_t)sit * slots * WH * d.esize), (uint64_t)nimg * WH * d.esize,
-                                 d.comp->v()), "upload");
-                const void *pdp = lplh ? pd.p : pd.at((uint64_t)sit * Pc * M * PDB);
-                const uint32_t npd = lplh ? (uint32_t)d.pd_all.size() : (uint32_t)(Pc * M);
-                auto slab_launch = [&](int64_t j) {
-                    const int32_t y0 = (int32_t)(j * slab), y1 = (int32_t)std::min<int64_t>(Hv, (j + 1) * slab);
-                    xpr_launch L = d.launch(y0, y1, origin, go_.vx, (uint32_t)d.Hd, 0, (uint32_t)(lplh ? slots : Pc), 0);
-                    if (lplh) {
-                        L.list_mvp = (const uint16_t *)lm.at((uint64_t)sit * slots * M * 2);
-                        L.list_img = (const uint16_t *)li.at((uint64_t)sit * slots * M * 2);
-                        L.n_list = (uint32_t)(nimg * M);
+        double t1 = 0.0;
+        if (sync_mode) {
+            // method_1a (reconstruction_lpln.hpp:27-96): one slab buffer, every transfer
+            // synchronous with the projector
+            const uint64_t avail = d.available();
+            const uint64_t budget = avail > (64ull << 20) ? avail - (64ull << 20) : layer_bytes;
+            int64_t slab = std::max<int64_t>(1, std::min<int64_t>(Hv, (int64_t)(budget / layer_bytes)));
+            if (p.slab > 0) slab = std::min<int64_t>(slab, p.slab);
+            DevBuf sb(d.ctx, (uint64_t)slab * layer_bytes);
+            std::cout << "Executing reconstruction..." << std::flush;
+            t1 = now();
+            float weight = p.weight;
+            const int64_t nslab = (Hv + slab - 1) / slab;
+            for (int64_t mit = 0; mit < p.it; ++mit) {
+                for (int64_t sit = 0; sit < S; ++sit) {
+                    d.jittered_origin(go_, origin);
+                    const bool first = (mit == 0 && sit == 0);
+                    check(xpr_upload(d.ctx, img.p, himg.at((uint64_t)sit * slots * WH * d.esize),
+                                     (uint64_t)Pc * WH * d.esize, d.comp->v()), "upload");
+                    const void *pdp = pd.at((uint64_t)sit * Pc * M * PDB);
+                    if (!first) {
+                        for (int64_t j = 0; j < nslab; ++j) {
+                            const int64_t y0 = j * slab, ny = std::min<int64_t>(Hv, (j + 1) * slab) - y0;
+                            check(xpr_upload(d.ctx, sb.p, hvol.at((uint64_t)y0 * layer_bytes),
+                                             (uint64_t)ny * layer_bytes, d.comp->v()), "upload");
+                            xpr_launch L = d.launch((int32_t)y0, (int32_t)(y0 + ny), origin, go_.vx, (uint32_t)d.Hd,
+                                                    0, (uint32_t)Pc, 0);
+                            check(xpr_forward(d.ctx, sb.as<float>(), sum.as<uint32_t>(), (const xpr_projdata *)pdp,
+                                              (uint32_t)(Pc * M), &L, d.comp->v()), "forward");
+                            stats_.pairs += (uint64_t)ny * W * W * Pc;
+                        }
                     }
-                    return L;
-                };
-                // ---- forward over the slabs (reconstruction_lpla.hpp:86-103)
-                if (!first) {
-                    if (lplh) check(xpr_fill_u32(d.ctx, sum.p, 0u, (uint64_t)slots * WH, d.comp->v()), "fill");
+                    check(xpr_error(d.ctx, img.p, d.dtype, sum.as<uint32_t>(), sep ? ratio.p : sum.p, d.dtype,
+                                    (uint64_t)Pc * WH, weight, XPR_ERROR_STD, 0, nullptr, d.comp->v()), "error");
                     for (int64_t j = 0; j < nslab; ++j) {
-                        const int b = (int)(j % nbuf);
                         const int64_t y0 = j * slab, ny = std::min<int64_t>(Hv, (j + 1) * slab) - y0;
-                        const Stream &cs = sync_mode ? *d.comp : *d.up;
-                        if (!sync_mode) e_done[b].wait_in(cs);
-                        check(xpr_upload(d.ctx, sb[b].p, hvol.at((uint64_t)y0 * layer_bytes), (uint64_t)ny * layer_bytes,
-                                         cs.v()), "upload");
-                        if (!sync_mode) { e_up[b].record(cs); e_up[b].wait_in(*d.comp); }
-                        xpr_launch L = slab_launch(j);
-                        check(xpr_forward(d.ctx, sb[b].as<float>(), sum.as<uint32_t>(), (const xpr_projdata *)pdp, npd,
-                                          &L, d.comp->v()), "forward");
-                        if (!sync_mode) e_done[b].record(*d.comp);
-                        stats_.pairs += (uint64_t)ny * W * W * nimg;
-                    }
-                }
-                // ---- error
-                const int mode = lplh ? (first ? XPR_ERROR_FIRST_1C : XPR_ERROR_1C) : XPR_ERROR_STD;
-                check(xpr_error(d.ctx, img.p, d.dtype, sum.as<uint32_t>(), sep ? ratio.p : sum.p, d.dtype,
-                                (uint64_t)nimg * WH, weight, mode, 0, nullptr, d.comp->v()), "error");
-                // ---- backward over the slabs, results back to the host volume
-                for (int64_t j = 0; j < nslab; ++j) {
-                    const int b = (int)(j % nbuf);
-                    const int64_t y0 = j * slab, ny = std::min<int64_t>(Hv, (j + 1) * slab) - y0;
-                    if (sync_mode) {
-                        check(xpr_upload(d.ctx, sb[b].p, hvol.at((uint64_t)y0 * layer_bytes), (uint64_t)ny * layer_bytes,
+                        check(xpr_upload(d.ctx, sb.p, hvol.at((uint64_t)y0 * layer_bytes), (uint64_t)ny * layer_bytes,
                                          d.comp->v()), "upload");
-                    } else {
-                        e_free[b].wait_in(*d.up);
-                        e_done[b].wait_in(*d.up);
-                        check(xpr_upload(d.ctx, sb[b].p, hvol.at((uint64_t)y0 * layer_bytes), (uint64_t)ny * layer_bytes,
-                                         d.up->v()), "upload");
-                        e_up[b].record(*d.up);
-                        e_up[b].wait_in(*d.comp);
+                        xpr_launch L = d.launch((int32_t)y0, (int32_t)(y0 + ny), origin, go_.vx, (uint32_t)d.Hd, 0,
+                                                (uint32_t)Pc, 0);
+                        check(xpr_backward(d.ctx, sb.as<float>(), sep ? ratio.p : sum.p, d.dtype,
+                                           (const xpr_projdata *)pdp, (uint32_t)(Pc * M), &L, d.comp->v()),
+                              "backward");
+                        stats_.pairs += (uint64_t)ny * W * W * Pc;
+                        check(xpr_download(d.ctx, hvol.at((uint64_t)y0 * layer_bytes), sb.p,
+                                           (uint64_t)ny * layer_bytes, d.comp->v()), "download");
                     }
-                    xpr_launch L = slab_launch(j);
-                    L.nan_skip = lplh ? 1 : 0;
-                    check(xpr_backward(d.ctx, sb[b].as<float>(), sep ? ratio.p : sum.p, d.dtype, (const xpr_projdata *)pdp,
-                                       npd, &L, d.comp->v()), "backward");
-                    stats_.pairs += (uint64_t)ny * W * W * nimg;
-                    if (sync_mode) {
-                        check(xpr_download(d.ctx, hvol.at((uint64_t)y0 * layer_bytes), sb[b].p, (uint64_t)ny * layer_bytes,
-                                           d.comp->v()), "download");
-                    } else {
-                        e_done[b].record(*d.comp);
-                        e_done[b].wait_in(*d.down);
-                        check(xpr_download(d.ctx, hvol.at((uint64_t)y0 * layer_bytes), sb[b].p, (uint64_t)ny * layer_bytes,
-                                           d.down->v()), "download");
-                        e_free[b].record(*d.down);
-                    }
+                    check(xpr_fill_u32(d.ctx, sum.p, 0u, (uint64_t)slots * WH, d.comp->v()), "fill");
+                    d.comp->sync();
+                    stats_.subiterations++;
                 }
-                if (!sync_mode) {
-                    // the next sub-iteration's forward reads the updated host volume
-                    d.down->sync();
-                    d.up->sync();
-                }
-                if (!lplh) check(xpr_fill_u32(d.ctx, sum.p, 0u, (uint64_t)slots * WH, d.comp->v()), "fill");
-                d.comp->sync();
-                stats_.subiterations++;
+                weight *= p.weight_factor;
             }
-            weight *= p.weight_factor;
+        } else {
+            // method_1b / 1c (reconstruction_lpla.hpp:29-157, reconstruction_lplh.hpp:40-219) with
+            // the volume's slabs kept in a device cache: as many slab buffers as the memory left
+            // beside the images holds (all of them when the volume fits), forward passes in
+            // ascending and backward passes in descending slab order so that each pass starts
+            // on the slabs the previous one left resident, a slab written back to the host
+            // only when its buffer is needed for another.  Uploads and write-backs run on
+            // their own streams, ordered against the projector by events.
+            const uint64_t avail = d.available();
+            const uint64_t budget = avail > (64ull << 20) ? avail - (64ull << 20) : layer_bytes;
+            int64_t slab = std::max<int64_t>(1, std::min<int64_t>(Hv, (int64_t)(budget / 8 / layer_bytes)));
+            if (p.slab > 0) slab = std::min<int64_t>(slab, p.slab);
+            const int64_t nslab = (Hv + slab - 1) / slab;
+            int64_t nb = std::max<int64_t>(1, std::min<int64_t>(nslab, (int64_t)(budget / (slab * layer_bytes))));
+            if (p.slab_cache > 0) nb = std::min<int64_t>(nb, p.slab_cache);
+            struct SlabBuf {
+                DevBuf mem;
+                int64_t slab = -1;
+                bool dirty = false, used_rec = false, saved_rec = false;
+                uint64_t last = 0;
+                Event ready, used, saved;
+            };
+            std::vector<std::unique_ptr<SlabBuf>> bufs;
+            for (int64_t b = 0; b < nb; ++b) {
+                bufs.emplace_back(std::make_unique<SlabBuf>());
+                bufs.back()->mem = DevBuf(d.ctx, (uint64_t)slab * layer_bytes);
+            }
+            Event last_save;
+            bool any_save = false;
+            uint64_t clock = 0;
+            auto extent = [&](int64_t j) {
+                const int64_t y0 = j * slab;
+                return std::make_pair(y0, std::min<int64_t>(Hv, y0 + slab) - y0);
+            };
+            auto write_back = [&](SlabBuf &b) {
+                const auto [y0, ny] = extent(b.slab);
+                if (b.used_rec) b.used.wait_in(*d.down);
+                check(xpr_download(d.ctx, hvol.at((uint64_t)y0 * layer_bytes), b.mem.p, (uint64_t)ny * layer_bytes,
+                                   d.down->v()), "download");
+                b.saved.record(*d.down);
+                b.saved_rec = true;
+                last_save.record(*d.down);
+                any_save = true;
+                b.dirty = false;
+            };
+            auto acquire = [&](int64_t j) -> SlabBuf & {
+                SlabBuf *v = nullptr;
+                for (auto &b : bufs)
+                    if (b->slab == j) v = b.get();
+                if (!v) {  // load slab j into the least recently used buffer
+                    for (auto &b : bufs)
+                        if (!v || b->slab < 0 || (v->slab >= 0 && b->last < v->last)) v = b.get();
+                    if (v->slab >= 0 && v->dirty) write_back(*v);
+                    if (v->used_rec) v->used.wait_in(*d.up);
+                    if (v->saved_rec) v->saved.wait_in(*d.up);
+                    if (any_save) last_save.wait_in(*d.up);  // the host copy of slab j is current
+                    const auto [y0, ny] = extent(j);
+                    check(xpr_upload(d.ctx, v->mem.p, hvol.at((uint64_t)y0 * layer_bytes), (uint64_t)ny * layer_bytes,
+                                     d.up->v()), "upload");
+                    v->ready.record(*d.up);
+                    v->ready.wait_in(*d.comp);
+                    v->slab = j;
+                    v->dirty = false;
+                }
+                v->last = ++clock;
+                return *v;
+            };
+            std::cout << "Executing reconstruction..." << std::flush;
+            t1 = now();
+            float weight = p.weight;
+            for (int64_t mit = 0; mit < p.it; ++mit) {
+                for (int64_t sit = 0; sit < S; ++sit) {
+                    d.jittered_origin(go_, origin);
+                    const bool first = (mit == 0 && sit == 0);
+                    const int64_t nimg = lplh ? d.angles_in(sit) : Pc;
+                    check(xpr_upload(d.ctx, img.p, himg.at((uint64_t)sit * slots * WH * d.esize),
+                                     (uint64_t)nimg * WH * d.esize, d.comp->v()), "upload");
+                    const void *pdp = lplh ? pd.p : pd.at((uint64_t)sit * Pc * M * PDB);
+                    const uint32_t npd = lplh ? (uint32_t)d.pd_all.size() : (uint32_t)(Pc * M);
+                    auto slab_launch = [&](int64_t j) {
+                        const auto [y0, ny] = extent(j);
+                        xpr_launch L = d.launch((int32_t)y0, (int32_t)(y0 + ny), origin, go_.vx, (uint32_t)d.Hd, 0,
+                                                (uint32_t)(lplh ? slots : Pc), 0);
+                        if (lplh) {
+                            L.list_mvp = (const uint16_t *)lm.at((uint64_t)sit * slots * M * 2);
+                            L.list_img = (const uint16_t *)li.at((uint64_t)sit * slots * M * 2);
+                            L.n_list = (uint32_t)(nimg * M);
+                        }
+                        return L;
+                    };
+                    // ---- forward over the slabs, ascending (reconstruction_lpla.hpp:86-103)
+                    if (!first) {
+                        if (lplh) check(xpr_fill_u32(d.ctx, sum.p, 0u, (uint64_t)slots * WH, d.comp->v()), "fill");
+                        for (int64_t j = 0; j < nslab; ++j) {
+                            SlabBuf &b = acquire(j);
+                            xpr_launch L = slab_launch(j);
+                            check(xpr_forward(d.ctx, b.mem.as<float>(), sum.as<uint32_t>(), (const xpr_projdata *)pdp,
+                                              npd, &L, d.comp->v()), "forward");
+                            b.used.record(*d.comp);
+                            b.used_rec = true;
+                            stats_.pairs += (uint64_t)extent(j).second * W * W * nimg;
+                        }
+                    }
+                    // ---- error
+                    const int mode = lplh ? (first ? XPR_ERROR_FIRST_1C : XPR_ERROR_1C) : XPR_ERROR_STD;
+                    check(xpr_error(d.ctx, img.p, d.dtype, sum.as<uint32_t>(), sep ? ratio.p : sum.p, d.dtype,
+                                    (uint64_t)nimg * WH, weight, mode, 0, nullptr, d.comp->v()), "error");
+                    // ---- backward over the slabs, descending
+                    for (int64_t j = nslab - 1; j >= 0; --j) {
+                        SlabBuf &b = acquire(j);
+                        xpr_launch L = slab_launch(j);
+                        L.nan_skip = lplh ? 1 : 0;
+                        check(xpr_backward(d.ctx, b.mem.as<float>(), sep ? ratio.p : sum.p, d.dtype,
+                                           (const xpr_projdata *)pdp, npd, &L, d.comp->v()), "backward");
+                        b.used.record(*d.comp);
+                        b.used_rec = true;
+                        b.dirty = true;
+                        stats_.pairs += (uint64_t)extent(j).second * W * W * nimg;
+                    }
+                    if (!lplh) check(xpr_fill_u32(d.ctx, sum.p, 0u, (uint64_t)slots * WH, d.comp->v()), "fill");
+                    stats_.subiterations++;
+                }
+                weight *= p.weight_factor;
+            }
+            for (auto &b : bufs)
+                if (b->slab >= 0 && b->dirty) write_back(*b);
+            d.comp->sync();
+            d.up->sync();
+            d.down->sync();
         }
         stats_.seconds_iterations = now() - t1;
         std::cout << "Ok" << std::endl;

@@ -114,6 +114,7 @@ Params params_from_json(const json::Value &root)
     });
     opt(r, "device", [&](const json::Value &v) { p.device = (int)num(v, "device"); });
     opt(r, "slab", [&](const json::Value &v) { p.slab = (int64_t)num(v, "slab"); });
+    opt(r, "slab_cache", [&](const json::Value &v) { p.slab_cache = (int64_t)num(v, "slab_cache"); });
 
     const json::Value *g = root.get("geometry");
     opt(g, "so", [&](const json::Value &v) { p.so = (float)num(v, "so"); });
@@ -206,7 +207,7 @@ std::string params_to_json(const Params &p)
     if (p.seed_set) o << ",\"seed\":" << p.seed;
     o << ",\"arith\":\"" << p.arith << "\",\"storage\":\"" << p.storage << "\",\"geometry\":\"" << p.geometry
       << "\",\"compat_pad\":" << b(p.compat_pad) << ",\"mem_cap\":" << p.mem_cap << ",\"device\":" << p.device
-      << ",\"slab\":" << p.slab << "}";
+      << ",\"slab\":" << p.slab << ",\"slab_cache\":" << p.slab_cache << "}";
     o << ",\"geometry\":{\"so\":" << fnum(p.so) << ",\"sd\":" << fnum(p.sd) << ",\"angle\":" << fnum(p.angle)
       << ",\"heli_offset\":" << fnum(p.heli_offset) << ",\"heli_step\":" << fnum(p.heli_step) << ",\"angle_list\":[";
     for (size_t i = 0; i < p.angle_list.size(); ++i) o << (i ? "," : "") << fnum(p.angle_list[i]);

@@ -13,6 +13,7 @@
 //   recon.mem_cap        device-memory cap, bytes or "64G" / "512M"
 //   recon.device         CUDA device ordinal
 //   recon.slab           layers per streamed y-slab in method_1a/1b/1c (0: as many as fit)
+//   recon.slab_cache     slabs method_1b/1c keep on the device (0: as many as the memory holds)
 //   recon.images_preproc alias of recon.normalize (the README's name for it)
 //   detector.modules[]   per-module {offset_x, offset_y, offset_z, roll, pitch, yaw}
 //                        (the reference's commented-out global_parameters.hpp:38-44, 51)
@@ -76,6 +77,7 @@ struct Params {
     uint64_t mem_cap = 0;
     int device = 0;
     int64_t slab = 0;
+    int64_t slab_cache = 0;
 };
 
 const char *method_name(Method m);
