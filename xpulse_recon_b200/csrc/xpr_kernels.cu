@@ -177,6 +177,30 @@ __device__ __forceinline__ uint32_t fdist(float y, uint32_t base)
     return __float_as_uint(__fadd_rz(y, 8388608.0f)) - base;
 }
 
+// Two lanes of IEEE single-precision arithmetic in one instruction (sm_100 packed f32x2):
+// each half is rounded exactly as the scalar operation, so results are unchanged.
+__device__ __forceinline__ void fma_rn2(float &d0, float &d1, float a0, float a1, float b, float c)
+{
+    asm("{.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %4};\n\t"
+        "mov.b64 rc, {%5, %5};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+        "mov.b64 {%0, %1}, rd;}"
+        : "=f"(d0), "=f"(d1)
+        : "f"(a0), "f"(a1), "f"(b), "f"(c));
+}
+__device__ __forceinline__ void add_rz2(float &d0, float &d1, float a0, float a1, float b)
+{
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %4};\n\t"
+        "add.rz.f32x2 rd, ra, rb;\n\t"
+        "mov.b64 {%0, %1}, rd;}"
+        : "=f"(d0), "=f"(d1)
+        : "f"(a0), "f"(a1), "f"(b));
+}
+
 // Column walker.  For the voxel column (ax, az) and y-positions py[0..LEN), calls
 // f(inside, k, in, idx) with idx the target index of ProjMeta.  Untilted projections
 // (flags.z) hoist u, w and 1/w out of the column; the others evaluate the full
@@ -205,10 +229,15 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
                 const float rw = __frcp_rn(Cw);
                 const uint32_t K = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x) + Kv;
                 const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
+                static_assert(LEN % 2 == 0, "columns are walked two voxels at a time");
 #pragma unroll
-                for (int k = 0; k < LEN; ++k)
-                    f(std::true_type{}, k, true,
-                      __float_as_uint(__fadd_rz(__fmaf_rn(py[k], Qv, Rv), 8388608.0f)) * pitch + K);
+                for (int k = 0; k < LEN; k += 2) {
+                    float y0, y1, b0, b1;
+                    fma_rn2(y0, y1, py[k], py[k + 1], Qv, Rv);
+                    add_rz2(b0, b1, y0, y1, 8388608.0f);
+                    f(std::true_type{}, k, true, __float_as_uint(b0) * pitch + K);
+                    f(std::true_type{}, k + 1, true, __float_as_uint(b1) * pitch + K);
+                }
             } else {
 #pragma unroll
                 for (int k = 0; k < LEN; ++k) {
