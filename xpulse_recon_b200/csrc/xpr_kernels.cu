@@ -200,6 +200,52 @@ __device__ __forceinline__ void add_rz2(float &d0, float &d1, float a0, float a1
         : "=f"(d0), "=f"(d1)
         : "f"(a0), "f"(a1), "f"(b));
 }
+__device__ __forceinline__ void fma_rn2v(float &d0, float &d1, float a0, float a1, float b0, float b1, float c0,
+                                         float c1)
+{
+    asm("{.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+        "mov.b64 {%0, %1}, rd;}"
+        : "=f"(d0), "=f"(d1)
+        : "f"(a0), "f"(a1), "f"(b0), "f"(b1), "f"(c0), "f"(c1));
+}
+__device__ __forceinline__ void mul_rn2v(float &d0, float &d1, float a0, float a1, float b0, float b1)
+{
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\t"
+        "mov.b64 {%0, %1}, rd;}"
+        : "=f"(d0), "=f"(d1)
+        : "f"(a0), "f"(a1), "f"(b0), "f"(b1));
+}
+// FAST contract for two voxels of a tilted column: the pixel coordinates' bits
+// fadd_rz(y, 2^23) for u (bu0, bu1) and v (bv0, bv1), with
+// rw = 1/fma(c_w.y, py, C_w), yu = fma(py, c_u.y*rw, fma(C_u, rw, 1/2)),
+// yv = fma(py, c_v.y*rw, fma(C_v, rw, 1/2 - off)).
+__device__ __forceinline__ void tilted_pair(float py0, float py1, float4 cu, float4 cv, float4 cw, float Cu, float Cv,
+                                            float Cw, float hv, uint32_t &bu0, uint32_t &bu1, uint32_t &bv0,
+                                            uint32_t &bv1)
+{
+    float w0, w1, t0, t1, i0, i1, y0, y1, b0, b1;
+    fma_rn2v(w0, w1, cw.y, cw.y, py0, py1, Cw, Cw);
+    const float rw0 = __frcp_rn(w0), rw1 = __frcp_rn(w1);
+    mul_rn2v(t0, t1, cu.y, cu.y, rw0, rw1);
+    fma_rn2v(i0, i1, Cu, Cu, rw0, rw1, 0.5f, 0.5f);
+    fma_rn2v(y0, y1, py0, py1, t0, t1, i0, i1);
+    add_rz2(b0, b1, y0, y1, 8388608.0f);
+    bu0 = __float_as_uint(b0);
+    bu1 = __float_as_uint(b1);
+    mul_rn2v(t0, t1, cv.y, cv.y, rw0, rw1);
+    fma_rn2v(i0, i1, Cv, Cv, rw0, rw1, hv, hv);
+    fma_rn2v(y0, y1, py0, py1, t0, t1, i0, i1);
+    add_rz2(b0, b1, y0, y1, 8388608.0f);
+    bv0 = __float_as_uint(b0);
+    bv1 = __float_as_uint(b1);
+}
 
 // Column walker.  For the voxel column (ax, az) and y-positions py[0..LEN), calls
 // f(inside, k, in, idx) with idx the target index of ProjMeta.  Untilted projections
@@ -239,12 +285,13 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
                     f(std::true_type{}, k + 1, true, __float_as_uint(b1) * pitch + K);
                 }
             } else {
+                const uint32_t Ku = Kv - fb.x;
 #pragma unroll
-                for (int k = 0; k < LEN; ++k) {
-                    const float rw = __frcp_rn(__fmaf_rn(cw.y, py[k], Cw));
-                    const uint32_t du = fdist(__fmaf_rn(py[k], __fmul_rn(cu.y, rw), __fmaf_rn(Cu, rw, 0.5f)), fb.x);
-                    const float yv = __fmaf_rn(py[k], __fmul_rn(cv.y, rw), __fmaf_rn(Cv, rw, hv));
-                    f(std::true_type{}, k, true, __float_as_uint(__fadd_rz(yv, 8388608.0f)) * pitch + du + Kv);
+                for (int k = 0; k < LEN; k += 2) {
+                    uint32_t bu0, bu1, bv0, bv1;
+                    tilted_pair(py[k], py[k + 1], cu, cv, cw, Cu, Cv, Cw, hv, bu0, bu1, bv0, bv1);
+                    f(std::true_type{}, k, true, bv0 * pitch + bu0 + Ku);
+                    f(std::true_type{}, k + 1, true, bv1 * pitch + bu1 + Ku);
                 }
             }
             return 2;
@@ -257,17 +304,22 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
             const uint32_t K = du + tgt.y;
             const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
 #pragma unroll
-            for (int k = 0; k < LEN; ++k) {
-                const uint32_t dv = fdist(__fmaf_rn(py[k], Qv, Rv), fb.z);
-                f(std::false_type{}, k, in_u && (dv < fb.w), dv * pitch + K);
+            for (int k = 0; k < LEN; k += 2) {
+                float y0, y1, b0, b1;
+                fma_rn2(y0, y1, py[k], py[k + 1], Qv, Rv);
+                add_rz2(b0, b1, y0, y1, 8388608.0f);
+                const uint32_t dv0 = __float_as_uint(b0) - fb.z, dv1 = __float_as_uint(b1) - fb.z;
+                f(std::false_type{}, k, in_u && (dv0 < fb.w), dv0 * pitch + K);
+                f(std::false_type{}, k + 1, in_u && (dv1 < fb.w), dv1 * pitch + K);
             }
         } else {
 #pragma unroll
-            for (int k = 0; k < LEN; ++k) {
-                const float rw = __frcp_rn(__fmaf_rn(cw.y, py[k], Cw));
-                const uint32_t du = fdist(__fmaf_rn(py[k], __fmul_rn(cu.y, rw), __fmaf_rn(Cu, rw, 0.5f)), fb.x);
-                const uint32_t dv = fdist(__fmaf_rn(py[k], __fmul_rn(cv.y, rw), __fmaf_rn(Cv, rw, hv)), fb.z);
-                f(std::false_type{}, k, (du < fb.y) && (dv < fb.w), dv * pitch + du + tgt.y);
+            for (int k = 0; k < LEN; k += 2) {
+                uint32_t bu0, bu1, bv0, bv1;
+                tilted_pair(py[k], py[k + 1], cu, cv, cw, Cu, Cv, Cw, hv, bu0, bu1, bv0, bv1);
+                const uint32_t du0 = bu0 - fb.x, du1 = bu1 - fb.x, dv0 = bv0 - fb.z, dv1 = bv1 - fb.z;
+                f(std::false_type{}, k, (du0 < fb.y) && (dv0 < fb.w), dv0 * pitch + du0 + tgt.y);
+                f(std::false_type{}, k + 1, (du1 < fb.y) && (dv1 < fb.w), dv1 * pitch + du1 + tgt.y);
             }
         }
     } else {
