@@ -75,7 +75,21 @@ def test_alone_equals_mixed(sctx, storage):
         assert np.isfinite(v).mean() > 0.5
         assert_same_bits(v, a)
     assert st.completed == len(reqs) and st.failed == 0
-    assert st.ticks < sum(p["recon"]["it"] * p["recon"]["sit"] for p, _ in reqs)  # requests shared ticks
+    srv.close()
+
+
+def test_requests_in_flight_share_ticks(sctx):
+    """Requests that arrive while others run join the running batch: 4 requests of 100
+    short sub-iterations each, submitted back to back, finish in far fewer than 400 ticks."""
+    srv = Server(sctx)
+    tickets = []
+    for i in range(4):
+        params, raw = _request(5)  # 20 projections of 16 x 24
+        params["recon"].update({"it": 5, "sit": 20, "seed": 500 + i})
+        tickets.append(srv.submit(params, raw))
+    assert all(srv.wait(t, 60.0).state == DONE for t in tickets)
+    st = srv.stats()
+    assert st.ticks < 4 * 100, st.ticks
     srv.close()
 
 
