@@ -12,10 +12,15 @@ px 0.1 mm, so 100, sd 1000, rx 1.5 px, sx -2, sy 3 (mm).  Data are synthetic
 forward projector, Poisson noise at 1e5 photons, -log preprocessing on the GPU).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--arith fast|strict] [--storage fp32|bf16|fp16] [--config c2|c1]
+                  [--arith fast|strict] [--storage fp32|bf16|fp16] [--shard]
+                  [--config c2|c1|c2slab|c3h|c4|c4one|c5]
 
 Under torchrun each rank reconstructs its own volume (weak scaling, no
-collective on the data path); the time is the max over ranks.
+collective on the data path), or with --shard one volume split into y-slabs over
+the ranks (strong scaling, one all-reduce of the detector sums per sub-iteration);
+the time is the max over ranks.  c3h runs whole reconstructions in every memory
+mode under a device-memory cap; c4 many small reconstructions as one batched run;
+c5 a request loop with Poisson arrivals (latency percentiles and served GUPS).
 """
 from __future__ import annotations
 
@@ -391,6 +396,11 @@ def cpu_baseline(cfg, seconds):
 # ----------------------------------------------------------------------------- main arms
 def run_reference(args, cfg, rank, world):
     if rank != 0:
+        return 0
+    if any(k not in cfg for k in ("so", "sd", "rx", "sx", "sy")):
+        emit({"impl": "reference", "unavailable": "the reference runs one reconstruction per process; %s is a "
+              "batched / served / out-of-core workload of this library (time its single-problem kernels with "
+              "--config c2)" % args.config})
         return 0
     step, info = cpu_reference_step_factory(cfg, max(1.0, min(10.0, 60.0 / max(1, args.steps + args.warmup))))
     for _ in range(args.warmup):
