@@ -13,13 +13,13 @@ forward projector, Poisson noise at 1e5 photons, -log preprocessing on the GPU).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--arith fast|strict] [--storage fp32|bf16|fp16] [--shard]
-                  [--config c2|c1|c2slab|c3h|c4|c4one|c5]
+                  [--config c2|c1|c2slab|c3h|c4|c4s|c4one|c5]
 
 Under torchrun each rank reconstructs its own volume (weak scaling, no
 collective on the data path), or with --shard one volume split into y-slabs over
 the ranks (strong scaling, one all-reduce of the detector sums per sub-iteration);
 the time is the max over ranks.  c3h runs whole reconstructions in every memory
-mode under a device-memory cap; c4 many small reconstructions as one batched run;
+mode under a device-memory cap; c4 / c4s many reconstructions as one batched run;
 c5 a request loop with Poisson arrivals (latency percentiles and served GUPS).
 """
 from __future__ import annotations
@@ -69,6 +69,12 @@ CONFIGS = {
                 outofcore=True, dwidth=1536, dheight=1024, projections=1000, sit=20, it=1, px=0.1, so=100.0,
                 sd=1000.0, phantom=1024, ellipsoids=60, background=0.0, i0=5e4, seed=3, mem_cap=8 << 30,
                 methods=["naive", "method_1b", "method_1c", "method_2"]),
+    # the batched form where it matters: reconstructions too small to fill the GPU alone
+    "c4s": dict(desc="256 small independent reconstructions: 96x64 detector on 3 modules of 32 px (roll/pitch/yaw "
+                     "U[-2,2] deg) -> 96x64x96 grid, 180 projections, sit=10 -> 18, it=2, so U[80,120], "
+                     "sd U[800,1200], BF16 image/ratio storage, batched persistent launches in a CUDA graph",
+                batch=256, dwidth=96, dheight=64, projections=180, sit=10, it=2, modules=3, px=0.1, rpy=2.0,
+                phantom=56, ellipsoids=6, background=0.0, i0=1e5, seed=6, plain_sample=16),
     # one problem of the c4 family (profiling-sized)
     "c4one": dict(desc="one 384^3 recon grid of the c4 family (3 tilted modules, 36 projections per sub-iteration)",
                   batch=1, dwidth=384, dheight=384, projections=360, sit=10, it=2, modules=3, px=0.1, rpy=2.0,
