@@ -559,6 +559,7 @@ def run_ours(args, cfg, rank, world, local):
         "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": 8},
         "gpu_launches": 3 * K,
         "kernels_ms": {"forward": f_ms, "error": statistics.mean(err), "backward": b_ms},
+        "kernel_gups": {"forward": pairs_step / (f_ms / 1000.0) / 1e9, "backward": pairs_step / (b_ms / 1000.0) / 1e9},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
                      "algorithmic_bytes": alg_bytes,
