@@ -264,6 +264,10 @@ void finish_request(xpr_server *s, Request *r)
     if (e != cudaSuccess && !err) err = XPR_ERR_CUDA;
     if (r->arena) cudaFreeAsync(r->arena, s->dl);
     r->arena = nullptr;
+    // a finished request keeps only what xpr_serve_poll reports
+    std::vector<xpr_projdata>().swap(r->pd_sub);
+    r->pp.origin = std::vector<float>();
+    r->pp.weight = std::vector<float>();
     std::lock_guard<std::mutex> lk(s->mu);
     s->bytes_in_use -= r->bytes;
     r->done_s = now_s(s->t0);
