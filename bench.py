@@ -842,6 +842,44 @@ def run_serving(args, cfg, rank, world, local):
         plain_pairs += pairs_of[k] * cfg["it"]
         assert rc == 0
     plain = plain_pairs / plain_s / 1e9
+
+    # the plain FP32 path under the same arrivals: one request at a time, first come first
+    # served, each through xpr_reconstruct_host (the reference's one-scan-per-run model)
+    def plain_open_loop():
+        import queue
+        import threading
+        jobs, lat = queue.Queue(), []
+
+        def worker():
+            while True:
+                item = jobs.get()
+                if item is None:
+                    return
+                t_sub, params, k = item
+                raw, N = data[k]
+                P, H, W = raw.shape
+                out = out_of[k]
+                rc = L.xpr_reconstruct_host(json.dumps(params).encode(), raw.ctypes.data, P, W, H, out.ctypes.data,
+                                            out.size, C.byref(C.c_double()))
+                lat.append(time.perf_counter() - t_sub if rc == 0 else float("nan"))
+
+        th = threading.Thread(target=worker)
+        th.start()
+        t0 = time.perf_counter()
+        for i, (params, k) in enumerate(reqs):
+            dt = arrivals[i] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            jobs.put((time.perf_counter(), params, k))
+        jobs.put(None)
+        th.join()
+        span = time.perf_counter() - t0
+        lat = np.array(lat)
+        return {"ok": bool(np.isfinite(lat).all()), "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
+                "gups": total_pairs / span / 1e9, "makespan_s": span}
+
+    res["plain_fp32"] = {"open_loop": plain_open_loop()}
     best = res["bf16"]["saturated"]["gups"]
     line = {"metric": "GUPS served (voxel x projection pairs / s), with p50 / p99 request latency",
             "value": best, "unit": "GUPS", "n_gpus": world, "steps": n, "warmup": 1,
