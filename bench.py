@@ -127,7 +127,8 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % os.getpid())
+        import tempfile
+        self.path = os.path.join(tempfile.gettempdir(), "xpr_clocks_%d.csv" % os.getpid())
 
     def start(self):
         try:
