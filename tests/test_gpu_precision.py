@@ -41,6 +41,9 @@ WORKLOADS = {
     # the 768^2 / 720-projection offset geometry at quarter scale, it 3, sit 10
     "offsets192_it3": (dict(dwidth=192, dheight=192, projections=180, rx=1.5, sx=-2.0, sy=3.0), 3, 10, 40,
                        2.0 / 3.0, 2),
+    # three modules of 64 px tilted by roll / pitch / yaw (the batched workload's detector), it 2
+    "modules3_rpy": (dict(dwidth=192, dheight=128, projections=180, module_number=3,
+                          mod_rpy=[1.5, -1.0, 0.5, -0.5, 1.2, -1.8, 0.9, 0.4, -1.1]), 2, 10, 20, 0.6, 3),
 }
 
 
@@ -66,23 +69,24 @@ def _phantom(W, Hv, n_ell, frac, rng):
     return vol
 
 
-def _projections(ctx, vol, pd_all, g, det, rng, i0=1e5, jitters=4):
+def _projections(ctx, vol, pd_all, g, det, rng, i0=1e5, jitters=4, modules=1):
     """Raw intensities I / I0 of the phantom: the average of `jitters` jittered GPU
     forward projections (all P angles), then Poisson noise at i0 photons per pixel."""
     W, Hv, P = int(g["vwidth"]), int(g["vheight"]), pd_all.shape[0]
     Wd, Hd = det
+    P_img = P // modules
     dvol = torch.from_numpy(vol.ravel()).cuda()
     dpd = torch.from_numpy(pd_all).cuda()
-    acc = np.zeros(P * Wd * Hd, np.float64)
+    acc = np.zeros(P_img * Wd * Hd, np.float64)
     r = Reconstruction(ctx, arith=_lib.FAST)
-    r.set_image_parameters(Wd, Hd, P)
+    r.set_image_parameters(Wd, Hd, P_img)
     r.set_volume_parameters((0, 0, 0), (W, Hv, W), [g["vx"]] * 3)
-    r.set_angle_number(P, 1)
+    r.set_angle_number(P // modules, modules)
     r.set_image_offset((0, Hd))
     r.set_projdata_buffer(dpd)
     r.set_volume_buffer(dvol)
     for _ in range(jitters):
-        sums = torch.zeros(P * Wd * Hd, dtype=torch.int32, device="cuda")
+        sums = torch.zeros(P_img * Wd * Hd, dtype=torch.int32, device="cuda")
         r._origin = tuple(float(np.float32(g["orig"][i]) + np.float32(rng.uniform(0, g["vx"]))) for i in range(3))
         r.set_sum_images_buffer(sums)
         r.forward()
@@ -90,7 +94,7 @@ def _projections(ctx, vol, pd_all, g, det, rng, i0=1e5, jitters=4):
         acc += sums.cpu().numpy().view(np.uint32).astype(np.float64) / 4194304.0
     p = acc / jitters
     counts = rng.poisson(i0 * np.exp(-p))
-    return (np.maximum(counts, 1) / i0).astype(np.float32).reshape(P, Hd, Wd)
+    return (np.maximum(counts, 1) / i0).astype(np.float32).reshape(P_img, Hd, Wd)
 
 
 def _product(raw, geom, it, sit, storage):
@@ -98,6 +102,11 @@ def _product(raw, geom, it, sit, storage):
                      "storage": storage, "mlog": True, "weight": 1.0, "weight_factor": 0.9},
            "geometry": {"so": 100.0, "sd": 1000.0, "angle": 360.0},
            "detector": {"px": 0.1, "rx": geom.get("rx", 0.0), "sx": geom.get("sx", 0.0), "sy": geom.get("sy", 0.0)}}
+    if "mod_rpy" in geom:
+        a = geom["mod_rpy"]
+        cfg["detector"]["module_number"] = geom["module_number"]
+        cfg["detector"]["modules"] = [{"roll": a[3 * m], "pitch": a[3 * m + 1], "yaw": a[3 * m + 2]}
+                                      for m in range(geom["module_number"])]
     L = _lib.lib()
     L.xpr_reconstruct_host.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.c_uint32, C.c_uint32, C.c_void_p,
                                        C.c_uint64, C.POINTER(C.c_double)]
@@ -139,7 +148,8 @@ def _workload(name):
         vol = _phantom(W, Hv, n_ell, frac, rng)
         ctx = Context(0)
         try:
-            raw = _projections(ctx, vol, pd_all, g, (geom["dwidth"], geom["dheight"]), rng)
+            raw = _projections(ctx, vol, pd_all, g, (geom["dwidth"], geom["dheight"]), rng,
+                               modules=geom.get("module_number", 1))
         finally:
             ctx.close()
         gp = O.geom_params(sit=sit, **geom)
@@ -159,7 +169,7 @@ def test_relative_rmse_against_fp64_oracle(name, storage):
     # of view may be reached in one precision and not in the other
     nan_mismatch = float(np.mean(np.isnan(v) != np.isnan(v64)))
     W = geom["dwidth"]
-    Hv = v.size // (W * W)
+    Hv = v.size // (W * W)  # the grid is dwidth x (dheight + helical extent) x dwidth
     err = _rel_rmse(v, v64, _region(W, Hv))
     err_all = _rel_rmse(v, v64)
     report = os.environ.get("XPR_PRECISION_REPORT")
