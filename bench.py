@@ -364,31 +364,37 @@ def cpu_reference_step_factory(cfg, seconds_target):
     origin = [float(np.float32(go.orig[i]) + np.float32(0.37 * go.vx)) for i in range(3)]
     y_mid = Hv // 2
 
-    def run(layers):
+    def run(layers, reps=1):
         y0 = y_mid - layers // 2
         n = W * layers * W
         vol = rng.uniform(1e-4, 3e-4, O.ndrange(n)).astype(np.float32)
-        sums = np.zeros(Pc * Wd * Hd, np.uint32)
         t = time.perf_counter()
-        if kind == "reference":
-            O.ref_forward(vol, sums, pd, Wd, Hd, origin, Pc, 1, (0, y0, 0), (W, y0 + layers, W), (0, Hd),
-                          [go.vx] * 3)
-            O.ref_error(images, sums, Wd, Hd, 1.0)
-            O.ref_backward(vol, sums.view(np.float32), pd, Wd, Hd, origin, Pc, 1, (0, y0, 0), (W, y0 + layers, W),
-                           (0, Hd), [go.vx] * 3)
-        else:
-            L, keep = O.make_launch((0, y0, 0), (W, y0 + layers, W), origin, [go.vx] * 3, Wd, Hd, 0, Pc, 1)
-            O.forward(vol, sums, pd, L)
-            O.error(images, sums, 1.0)
-            O.backward(vol, sums.view(np.float32), pd, L)
-        return time.perf_counter() - t, n * Pc
+        for _ in range(reps):
+            sums = np.zeros(Pc * Wd * Hd, np.uint32)
+            if kind == "reference":
+                O.ref_forward(vol, sums, pd, Wd, Hd, origin, Pc, 1, (0, y0, 0), (W, y0 + layers, W), (0, Hd),
+                              [go.vx] * 3)
+                O.ref_error(images, sums, Wd, Hd, 1.0)
+                O.ref_backward(vol, sums.view(np.float32), pd, Wd, Hd, origin, Pc, 1, (0, y0, 0),
+                               (W, y0 + layers, W), (0, Hd), [go.vx] * 3)
+            else:
+                L, keep = O.make_launch((0, y0, 0), (W, y0 + layers, W), origin, [go.vx] * 3, Wd, Hd, 0, Pc, 1)
+                O.forward(vol, sums, pd, L)
+                O.error(images, sums, 1.0)
+                O.backward(vol, sums.view(np.float32), pd, L)
+        return time.perf_counter() - t, n * Pc * reps
 
-    # calibrate on a few layers (one layer is dominated by fixed costs), then size the sample
+    # calibrate on a few layers (one layer is dominated by fixed costs), then size the sample:
+    # a slab of the grid, or the whole grid repeated when the grid is smaller than the target
     probe = min(8, Hv)
     dt, pairs = run(probe)
     layers = int(max(1, min(Hv, round(probe * seconds_target / max(dt, 1e-3)))))
-    info = {"kind": kind, "cores": os.cpu_count(), "layers": layers, "W": W, "Pc": Pc}
-    return (lambda: run(layers)), info
+    reps = 1
+    if layers == Hv:
+        dt_full, _ = run(Hv)
+        reps = int(max(1, round(seconds_target / max(dt_full, 1e-3))))
+    info = {"kind": kind, "cores": os.cpu_count(), "layers": layers, "W": W, "Pc": Pc, "reps": reps}
+    return (lambda: run(layers, reps)), info
 
 
 def cpu_baseline(cfg, seconds):
@@ -396,8 +402,9 @@ def cpu_baseline(cfg, seconds):
     dt, pairs = step()
     return {"value": pairs / dt / 1e9, "unit": "GUPS", "cores": info["cores"], "kind": info["kind"],
             "sample": "forward + error + backward of a %d-layer y-slab (%dx%dx%d voxels) against one "
-                      "sub-iteration's %d projections, OpenMP on %d host threads, %.1f s"
-                      % (info["layers"], info["W"], info["layers"], info["W"], info["Pc"], info["cores"], dt)}
+                      "sub-iteration's %d projections, %d time(s), OpenMP on %d host threads, %.1f s"
+                      % (info["layers"], info["W"], info["layers"], info["W"], info["Pc"], info["reps"],
+                         info["cores"], dt)}
 
 
 # ----------------------------------------------------------------------------- main arms
