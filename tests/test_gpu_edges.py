@@ -93,3 +93,28 @@ def test_null_buffers_are_refused(ctx):
     L = _lib.lib()
     d = _launch()
     assert L.xpr_forward(ctx.handle, None, None, None, 1, C.byref(d), None) == 1
+
+
+@pytest.mark.parametrize("nbytes", [4096, 48 << 20])
+def test_pinned_host_memory_round_trip(ctx, nbytes):
+    """xpr_alloc_pinned below and above the size at which large buffers are mapped with
+    huge pages and registered (32 MB): device copies on a stream run from and to it, it
+    holds what is written, and xpr_free_pinned releases it."""
+    L = _lib.lib()
+    hp, hq = C.c_void_p(), C.c_void_p()
+    _lib.check(L.xpr_alloc_pinned(ctx.handle, nbytes, C.byref(hp)), "alloc_pinned")
+    _lib.check(L.xpr_alloc_pinned(ctx.handle, nbytes, C.byref(hq)), "alloc_pinned")
+    try:
+        a = np.frombuffer((C.c_uint8 * nbytes).from_address(hp.value), np.uint8)
+        b = np.frombuffer((C.c_uint8 * nbytes).from_address(hq.value), np.uint8)
+        a[:] = np.random.default_rng(5).integers(0, 256, nbytes, dtype=np.uint8)
+        b[:] = 0
+        dev = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.check(L.xpr_upload(ctx.handle, dev.data_ptr(), hp, nbytes, s), "upload")
+        _lib.check(L.xpr_download(ctx.handle, hq, dev.data_ptr(), nbytes, s), "download")
+        _lib.check(L.xpr_synchronize(ctx.handle, s), "synchronize")
+        np.testing.assert_array_equal(a, b)
+    finally:
+        _lib.check(L.xpr_free_pinned(ctx.handle, hp), "free_pinned")
+        _lib.check(L.xpr_free_pinned(ctx.handle, hq), "free_pinned")

@@ -11,6 +11,7 @@
 #include <string>
 #include <unordered_map>
 
+#include "host/pinned.h"
 #include "xpr_internal.h"
 
 struct xpr_ctx {
@@ -183,11 +184,11 @@ int xpr_alloc_pinned(xpr_ctx *ctx, uint64_t bytes, void **hptr)
 {
     XPR_CHECK_CTX(ctx);
     if (!hptr) return fail(XPR_ERR_INVALID, "hptr is NULL");
-    cudaError_t e = cudaMallocHost(hptr, bytes ? bytes : 4);
+    cudaError_t e = xpr::pinned_alloc(hptr, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         *hptr = nullptr;
-        return cuda_fail(e, "cudaMallocHost");
+        return cuda_fail(e, "page-locked host allocation");
     }
     return XPR_OK;
 }
@@ -196,8 +197,8 @@ int xpr_free_pinned(xpr_ctx *ctx, void *hptr)
 {
     XPR_CHECK_CTX(ctx);
     if (!hptr) return XPR_OK;
-    cudaError_t e = cudaFreeHost(hptr);
-    return e == cudaSuccess ? XPR_OK : cuda_fail(e, "cudaFreeHost");
+    cudaError_t e = xpr::pinned_free(hptr);
+    return e == cudaSuccess ? XPR_OK : cuda_fail(e, "page-locked host release");
 }
 
 int xpr_upload(xpr_ctx *ctx, void *dst, const void *src, uint64_t bytes, void *stream)
