@@ -579,14 +579,15 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
     // thread = the voxel column (x0 + lane, z0 + warp), layers y0 .. y0 + CB
     const int ax = a.vmin[0] + x0 + lane, az = a.vmin[2] + z0 + warp;
 
-    float py[CB], s[CB];
+    // the column's y positions are the same for every thread: kept in shared memory
+    // (read as broadcasts), which leaves the registers to the sums and the gathers in flight
+    __shared__ __align__(16) float py[CB];
+    float s[CB];
     uint32_t n2[CB / 2];  // in-bounds counts, two 16-bit halves per word (k even: low, odd: high)
     uint32_t n_inside = 0;  // projections walked on the inside path: every voxel of the column counted
+    if (threadIdx.x < CB) py[threadIdx.x] = pos<ARITH>(a.vmin[1] + y0 + (int)threadIdx.x, a.voxel[1], a.origin[1]);
 #pragma unroll
-    for (int k = 0; k < CB; ++k) {
-        py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
-        s[k] = 0.0f;
-    }
+    for (int k = 0; k < CB; ++k) s[k] = 0.0f;
 #pragma unroll
     for (int k = 0; k < CB / 2; ++k) n2[k] = 0u;
 
@@ -649,7 +650,7 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
 
 
 template <int ARITH, bool LIST, bool NANSKIP, int DT, int CB>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, 4)
     k_backward_tiled(float *__restrict__ vol, const void *__restrict__ ratio, const xpr_projdata *__restrict__ pd,
                      const LaunchArgs a, int bricks_x, int bricks_z)
 {
