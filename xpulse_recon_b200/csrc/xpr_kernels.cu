@@ -844,7 +844,7 @@ __global__ void __launch_bounds__(NT, 4)
 }
 
 template <int ARITH, int DT, int CB>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, 4)
     k_backward_batched(const BatchBwdItem *__restrict__ items, int n_items, uint32_t total_units, uint32_t *ticket)
 {
     __shared__ ProjMeta s_meta[2 * G];
