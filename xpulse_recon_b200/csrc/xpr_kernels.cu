@@ -47,8 +47,8 @@ constexpr int BZ = 32;          // forward brick extent along z
 constexpr int NT = 256;         // threads per CTA (8 warps)
 constexpr int G = 4;            // projections whose tiles are in flight together
 constexpr int TILE_CAP = 1024;  // pixels per shared-memory tile
-constexpr int VSTRIDE = 66;     // padded row stride (words) of the brick value array: 32 x-positions of two
-                                // layers interleaved, + 2 (64-bit reads bank-conflict free both ways)
+constexpr int VSTRIDE = 132;    // padded row stride (words) of the brick value array: 32 x-positions of four
+                                // layers interleaved, + 4 (128-bit reads bank-conflict free both ways)
 constexpr int BWD_BY = 16;      // backward column length along y
 constexpr int BWD_BZ = 8;       // backward brick extent along z (one warp per z)
 constexpr uint32_t kMagic = 0x4B000000u;  // float bits of 2^23: bits(fadd_rz(y, 2^23)) - kMagic = floor(y)
@@ -361,7 +361,7 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
 // --------------------------------------------------------------------------------------
 // forward
 // --------------------------------------------------------------------------------------
-constexpr size_t kFwdSmem = (size_t)(BY / 2 * BZ * VSTRIDE + G * TILE_CAP) * sizeof(uint32_t);
+constexpr size_t kFwdSmem = (size_t)(BY / 4 * BZ * VSTRIDE + G * TILE_CAP) * sizeof(uint32_t);
 
 // One forward work unit: brick `brick` (x fastest, then z, then y) against the
 // projection run `split` (entries [split * per_split, (split + 1) * per_split)).
@@ -372,10 +372,10 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                                              uint32_t brick, uint32_t split, int bricks_x, int bricks_z,
                                              uint32_t *smem, ProjMeta *s_meta)
 {
-    // fixed-point values [BY / 2][BZ][VSTRIDE]: layers 2m and 2m + 1 of (x, z) are adjacent
-    // words, so a thread reads a pair of its column's voxels with one 64-bit load
+    // fixed-point values [BY / 4][BZ][VSTRIDE]: layers 4m .. 4m + 3 of (x, z) are adjacent
+    // words, so a thread reads four of its column's voxels with one 128-bit load
     uint32_t *s_val = smem;
-    uint32_t *s_tile = smem + BY / 2 * BZ * VSTRIDE;   // [G][TILE_CAP]
+    uint32_t *s_tile = smem + BY / 4 * BZ * VSTRIDE;   // [G][TILE_CAP]
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int b = (int)brick;
@@ -392,7 +392,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
         const int gx = x0 + x, gy = y0 + y, gz = z0 + z;
         uint32_t v = 0;
         if (gx < sx && gy < sy && gz < sz) v = float_to_fixed(__ldg(&vol[((size_t)gy * sz + gz) * sx + gx]));
-        s_val[((y >> 1) * BZ + z) * VSTRIDE + 2 * x + (y & 1)] = v;
+        s_val[((y >> 2) * BZ + z) * VSTRIDE + 4 * x + (y & 3)] = v;
         any |= (v != 0u);
     }
     for (int i = threadIdx.x; i < G * TILE_CAP; i += NT) s_tile[i] = 0u;
@@ -422,20 +422,20 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
             for (int j = 0; j < 4; ++j) {
                 const int cx = orx ? warp + 8 * j : lane;
                 const int cz = orx ? lane : warp + 8 * j;
-                const uint2 *vals = reinterpret_cast<const uint2 *>(s_val + cz * VSTRIDE + 2 * cx);
-                uint2 pair;
+                const uint4 *vals = reinterpret_cast<const uint4 *>(s_val + cz * VSTRIDE + 4 * cx);
+                uint4 quad;
                 const int ax = a.vmin[0] + x0 + cx, az = a.vmin[2] + z0 + cz;
                 if (fl.x == kTile) {
                     // a zero adds nothing to a shared-memory tile; no test for it
                     walk_column<ARITH, BY>(M, a, ax, az, py, [&](auto, int k, bool in, uint32_t idx) {
-                        if (!(k & 1)) pair = vals[(k >> 1) * (BZ * VSTRIDE / 2)];
-                        const uint32_t v = (k & 1) ? pair.y : pair.x;
+                        if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
+                        const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
                         if (in) atomicAdd(&tile[idx], v);
                     });
                 } else {
                     walk_column<ARITH, BY>(M, a, ax, az, py, [&](auto, int k, bool in, uint32_t idx) {
-                        if (!(k & 1)) pair = vals[(k >> 1) * (BZ * VSTRIDE / 2)];
-                        const uint32_t v = (k & 1) ? pair.y : pair.x;
+                        if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
+                        const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
                         if (in & (v != 0u)) atomicAdd(&sum[idx], v);
                     });
                 }
