@@ -248,6 +248,75 @@ __device__ __forceinline__ void tilted_pair(float py0, float py1, float4 cu, flo
     bv1 = __float_as_uint(b1);
 }
 
+// FAST-contract part of the column walker (below), from the column's numerators
+// C_u, C_v, C_w = fma(c.x, px, c.w) + c.z * pz; same calls and return value.
+template <int LEN, typename F>
+__device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a, float Cu, float Cv, float Cw,
+                                         const float (&py)[LEN], F &&f)
+{
+    const float4 cu = M.cu, cv = M.cv, cw = M.cw;
+    const uint4 tgt = M.tgt;
+    const uint32_t pitch = tgt.x;
+    const uint4 fb = M.fast;
+    const float hv = a.half_minus_off;
+    if (M.flags.w) {
+        // dv = bits(fadd_rz(yv, 2^23)) - fb.z is in [0, rows) for every voxel, so the
+        // index dv * pitch + du + off is bits * pitch + (du + off - fb.z * pitch) mod 2^32
+        const uint32_t Kv = tgt.y - fb.z * pitch;
+        if (M.flags.z) {
+            const float rw = __frcp_rn(Cw);
+            const uint32_t K = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x) + Kv;
+            const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
+            static_assert(LEN % 2 == 0, "columns are walked two voxels at a time");
+#pragma unroll
+            for (int k = 0; k < LEN; k += 2) {
+                float y0, y1, b0, b1;
+                fma_rn2(y0, y1, py[k], py[k + 1], Qv, Rv);
+                add_rz2(b0, b1, y0, y1, 8388608.0f);
+                f(std::true_type{}, k, true, __float_as_uint(b0) * pitch + K);
+                f(std::true_type{}, k + 1, true, __float_as_uint(b1) * pitch + K);
+            }
+        } else {
+            const uint32_t Ku = Kv - fb.x;
+#pragma unroll
+            for (int k = 0; k < LEN; k += 2) {
+                uint32_t bu0, bu1, bv0, bv1;
+                tilted_pair(py[k], py[k + 1], cu, cv, cw, Cu, Cv, Cw, hv, bu0, bu1, bv0, bv1);
+                f(std::true_type{}, k, true, bv0 * pitch + bu0 + Ku);
+                f(std::true_type{}, k + 1, true, bv1 * pitch + bu1 + Ku);
+            }
+        }
+        return 2;
+    }
+    if (M.flags.z) {
+        const float rw = __frcp_rn(Cw);
+        const uint32_t du = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x);
+        const bool in_u = du < fb.y;
+        if (!__any_sync(0xffffffffu, in_u)) return 0;
+        const uint32_t K = du + tgt.y;
+        const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
+#pragma unroll
+        for (int k = 0; k < LEN; k += 2) {
+            float y0, y1, b0, b1;
+            fma_rn2(y0, y1, py[k], py[k + 1], Qv, Rv);
+            add_rz2(b0, b1, y0, y1, 8388608.0f);
+            const uint32_t dv0 = __float_as_uint(b0) - fb.z, dv1 = __float_as_uint(b1) - fb.z;
+            f(std::false_type{}, k, in_u && (dv0 < fb.w), dv0 * pitch + K);
+            f(std::false_type{}, k + 1, in_u && (dv1 < fb.w), dv1 * pitch + K);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < LEN; k += 2) {
+            uint32_t bu0, bu1, bv0, bv1;
+            tilted_pair(py[k], py[k + 1], cu, cv, cw, Cu, Cv, Cw, hv, bu0, bu1, bv0, bv1);
+            const uint32_t du0 = bu0 - fb.x, du1 = bu1 - fb.x, dv0 = bv0 - fb.z, dv1 = bv1 - fb.z;
+            f(std::false_type{}, k, (du0 < fb.y) && (dv0 < fb.w), dv0 * pitch + du0 + tgt.y);
+            f(std::false_type{}, k + 1, (du1 < fb.y) && (dv1 < fb.w), dv1 * pitch + du1 + tgt.y);
+        }
+    }
+    return 1;
+}
+
 // Column walker.  For the voxel column (ax, az) and y-positions py[0..LEN), calls
 // f(inside, k, in, idx) with idx the target index of ProjMeta.  Untilted projections
 // (flags.z) hoist u, w and 1/w out of the column; the others evaluate the full
@@ -264,66 +333,9 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
     const float px = pos<ARITH>(ax, a.voxel[0], a.origin[0]);
     const float pz = pos<ARITH>(az, a.voxel[2], a.origin[2]);
     const uint32_t pitch = tgt.x;
-    if (ARITH == kFast) {
-        const uint4 fb = M.fast;
-        const float Cu = col_fast(cu, px, pz), Cv = col_fast(cv, px, pz), Cw = col_fast(cw, px, pz);
-        const float hv = a.half_minus_off;
-        if (M.flags.w) {
-            // dv = bits(fadd_rz(yv, 2^23)) - fb.z is in [0, rows) for every voxel, so the
-            // index dv * pitch + du + off is bits * pitch + (du + off - fb.z * pitch) mod 2^32
-            const uint32_t Kv = tgt.y - fb.z * pitch;
-            if (M.flags.z) {
-                const float rw = __frcp_rn(Cw);
-                const uint32_t K = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x) + Kv;
-                const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
-                static_assert(LEN % 2 == 0, "columns are walked two voxels at a time");
-#pragma unroll
-                for (int k = 0; k < LEN; k += 2) {
-                    float y0, y1, b0, b1;
-                    fma_rn2(y0, y1, py[k], py[k + 1], Qv, Rv);
-                    add_rz2(b0, b1, y0, y1, 8388608.0f);
-                    f(std::true_type{}, k, true, __float_as_uint(b0) * pitch + K);
-                    f(std::true_type{}, k + 1, true, __float_as_uint(b1) * pitch + K);
-                }
-            } else {
-                const uint32_t Ku = Kv - fb.x;
-#pragma unroll
-                for (int k = 0; k < LEN; k += 2) {
-                    uint32_t bu0, bu1, bv0, bv1;
-                    tilted_pair(py[k], py[k + 1], cu, cv, cw, Cu, Cv, Cw, hv, bu0, bu1, bv0, bv1);
-                    f(std::true_type{}, k, true, bv0 * pitch + bu0 + Ku);
-                    f(std::true_type{}, k + 1, true, bv1 * pitch + bu1 + Ku);
-                }
-            }
-            return 2;
-        }
-        if (M.flags.z) {
-            const float rw = __frcp_rn(Cw);
-            const uint32_t du = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x);
-            const bool in_u = du < fb.y;
-            if (!__any_sync(0xffffffffu, in_u)) return 0;
-            const uint32_t K = du + tgt.y;
-            const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
-#pragma unroll
-            for (int k = 0; k < LEN; k += 2) {
-                float y0, y1, b0, b1;
-                fma_rn2(y0, y1, py[k], py[k + 1], Qv, Rv);
-                add_rz2(b0, b1, y0, y1, 8388608.0f);
-                const uint32_t dv0 = __float_as_uint(b0) - fb.z, dv1 = __float_as_uint(b1) - fb.z;
-                f(std::false_type{}, k, in_u && (dv0 < fb.w), dv0 * pitch + K);
-                f(std::false_type{}, k + 1, in_u && (dv1 < fb.w), dv1 * pitch + K);
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < LEN; k += 2) {
-                uint32_t bu0, bu1, bv0, bv1;
-                tilted_pair(py[k], py[k + 1], cu, cv, cw, Cu, Cv, Cw, hv, bu0, bu1, bv0, bv1);
-                const uint32_t du0 = bu0 - fb.x, du1 = bu1 - fb.x, dv0 = bv0 - fb.z, dv1 = bv1 - fb.z;
-                f(std::false_type{}, k, (du0 < fb.y) && (dv0 < fb.w), dv0 * pitch + du0 + tgt.y);
-                f(std::false_type{}, k + 1, (du1 < fb.y) && (dv1 < fb.w), dv1 * pitch + du1 + tgt.y);
-            }
-        }
-    } else {
+    if (ARITH == kFast)
+        return walk_fast<LEN>(M, a, col_fast(cu, px, pz), col_fast(cv, px, pz), col_fast(cw, px, pz), py, f);
+    {  // STRICT
         const int4 rc = M.rect;
         const float off = a.row_off_f;
         if (M.flags.z) {
@@ -417,6 +429,46 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
             if (fl.x == kSkip) continue;
             uint32_t *tile = s_tile + g * TILE_CAP;
             const bool orx = fl.y;
+            if (ARITH == kFast && fl.x == kTile) {
+                // FAST into a tile: one lane coordinate is the thread's for all of its columns,
+                // so its share of the column numerators C = fma(c.x, px, c.w) + c.z * pz is
+                // computed once per projection
+                const float4 cu = M.cu, cv = M.cv, cw = M.cw;
+                auto splat = [&](const uint4 *vals, float Cu, float Cv, float Cw) {
+                    uint4 quad;
+                    // a zero adds nothing to a shared-memory tile; no test for it
+                    walk_fast<BY>(M, a, Cu, Cv, Cw, py, [&](auto, int k, bool in, uint32_t idx) {
+                        if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
+                        const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
+                        if (in) atomicAdd(&tile[idx], v);
+                    });
+                };
+                if (orx) {
+                    const float pz = pos<kFast>(a.vmin[2] + z0 + lane, a.voxel[2], a.origin[2]);
+                    const float Pu = __fmul_rn(cu.z, pz), Pv = __fmul_rn(cv.z, pz), Pw = __fmul_rn(cw.z, pz);
+#pragma unroll 1
+                    for (int j = 0; j < 4; ++j) {
+                        const int cx = warp + 8 * j;
+                        const float px = pos<kFast>(a.vmin[0] + x0 + cx, a.voxel[0], a.origin[0]);
+                        splat(reinterpret_cast<const uint4 *>(s_val + lane * VSTRIDE + 4 * cx),
+                              __fadd_rn(__fmaf_rn(cu.x, px, cu.w), Pu), __fadd_rn(__fmaf_rn(cv.x, px, cv.w), Pv),
+                              __fadd_rn(__fmaf_rn(cw.x, px, cw.w), Pw));
+                    }
+                } else {
+                    const float px = pos<kFast>(a.vmin[0] + x0 + lane, a.voxel[0], a.origin[0]);
+                    const float Au = __fmaf_rn(cu.x, px, cu.w), Av = __fmaf_rn(cv.x, px, cv.w),
+                                Aw = __fmaf_rn(cw.x, px, cw.w);
+#pragma unroll 1
+                    for (int j = 0; j < 4; ++j) {
+                        const int cz = warp + 8 * j;
+                        const float pz = pos<kFast>(a.vmin[2] + z0 + cz, a.voxel[2], a.origin[2]);
+                        splat(reinterpret_cast<const uint4 *>(s_val + cz * VSTRIDE + 4 * lane),
+                              __fadd_rn(Au, __fmul_rn(cu.z, pz)), __fadd_rn(Av, __fmul_rn(cv.z, pz)),
+                              __fadd_rn(Aw, __fmul_rn(cw.z, pz)));
+                    }
+                }
+                continue;
+            }
             // 4 columns per thread; lanes run across the ray so a warp hits distinct pixels
 #pragma unroll 1
             for (int j = 0; j < 4; ++j) {
@@ -425,7 +477,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 const uint4 *vals = reinterpret_cast<const uint4 *>(s_val + cz * VSTRIDE + 4 * cx);
                 uint4 quad;
                 const int ax = a.vmin[0] + x0 + cx, az = a.vmin[2] + z0 + cz;
-                if (fl.x == kTile) {
+                if (ARITH != kFast && fl.x == kTile) {
                     // a zero adds nothing to a shared-memory tile; no test for it
                     walk_column<ARITH, BY>(M, a, ax, az, py, [&](auto, int k, bool in, uint32_t idx) {
                         if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
