@@ -180,6 +180,7 @@ __device__ __forceinline__ uint32_t fdist(float y, uint32_t base)
 
 // Two lanes of IEEE single-precision arithmetic in one instruction (sm_100 packed f32x2):
 // each half is rounded exactly as the scalar operation, so results are unchanged.
+// Scalar-operand forms (each call pairs its operands); the forward's walk uses these.
 __device__ __forceinline__ void fma_rn2(float &d0, float &d1, float a0, float a1, float b, float c)
 {
     asm("{.reg .b64 ra, rb, rc, rd;\n\t"
@@ -248,8 +249,90 @@ __device__ __forceinline__ void tilted_pair(float py0, float py1, float4 cu, flo
     bv1 = __float_as_uint(b1);
 }
 
+// Register-pair forms: the operands are 64-bit pairs {lo, hi}, and values that stay packed
+// across a column (the y positions, the column constants) are paired once, not per
+// instruction; the backward's walk uses these.
+__device__ __forceinline__ uint64_t f2pack(float lo, float hi)
+{
+    uint64_t d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ void f2unpack(uint64_t v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ void u2unpack(uint64_t v, uint32_t &lo, uint32_t &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(v));
+}
+__device__ __forceinline__ float f2lo(uint64_t v)
+{
+    float lo, hi;
+    f2unpack(v, lo, hi);
+    return lo;
+}
+__device__ __forceinline__ float f2hi(uint64_t v)
+{
+    float lo, hi;
+    f2unpack(v, lo, hi);
+    return hi;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c)
+{
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t addrz2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("add.rz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+// y position of layer k of a column, from its pairs or from a plain array
+template <int N>
+__device__ __forceinline__ float ypos(const uint64_t (&py2)[N], int k)
+{
+    return (k & 1) ? f2hi(py2[k >> 1]) : f2lo(py2[k >> 1]);
+}
+template <int N>
+__device__ __forceinline__ float ypos(const float (&py)[N], int k)
+{
+    return py[k];
+}
+
+// Column constants of the FAST contract, each duplicated into both halves of a pair.
+struct Packed {
+    uint64_t magic;           // {2^23, 2^23}
+    uint64_t cuy, cvy, cwy;   // c.y of the u, v, w rows
+    uint64_t Cu, Cv, Cw;      // column numerators
+    uint64_t half, hv;        // {1/2, 1/2}, {1/2 - off, 1/2 - off}
+};
+
+// FAST contract for two voxels (py pair P) of a tilted column: the pixel coordinates'
+// bits fadd_rz(y, 2^23) for u (bu) and v (bv), each as {voxel 0, voxel 1}, with
+// rw = 1/fma(c_w.y, py, C_w), yu = fma(py, c_u.y*rw, fma(C_u, rw, 1/2)),
+// yv = fma(py, c_v.y*rw, fma(C_v, rw, 1/2 - off)).
+__device__ __forceinline__ void tilted_pair(uint64_t P, const Packed &k, uint64_t &bu, uint64_t &bv)
+{
+    float w0, w1;
+    f2unpack(fma2(k.cwy, P, k.Cw), w0, w1);
+    const uint64_t rw = f2pack(__frcp_rn(w0), __frcp_rn(w1));
+    bu = addrz2(fma2(P, mul2(k.cuy, rw), fma2(k.Cu, rw, k.half)), k.magic);
+    bv = addrz2(fma2(P, mul2(k.cvy, rw), fma2(k.Cv, rw, k.hv)), k.magic);
+}
+
 // FAST-contract part of the column walker (below), from the column's numerators
-// C_u, C_v, C_w = fma(c.x, px, c.w) + c.z * pz; same calls and return value.
+// C_u, C_v, C_w = fma(c.x, px, c.w) + c.z * pz; same calls and return value.  Two forms
+// of the same arithmetic: y positions as floats (this one, the forward's: measured faster
+// there) or in register pairs (the next one, the backward's: measured faster there).
 template <int LEN, typename F>
 __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a, float Cu, float Cv, float Cw,
                                          const float (&py)[LEN], F &&f)
@@ -317,16 +400,100 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
     return 1;
 }
 
-// Column walker.  For the voxel column (ax, az) and y-positions py[0..LEN), calls
+// FAST-contract part of the column walker (below), from the column's numerators
+// C_u, C_v, C_w = fma(c.x, px, c.w) + c.z * pz; same calls and return value.  py2 holds
+// the column's y positions in pairs {py[2m], py[2m + 1]}.
+template <int LEN, typename F>
+__device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a, float Cu, float Cv, float Cw,
+                                         const uint64_t (&py2)[LEN / 2], F &&f)
+{
+    static_assert(LEN % 2 == 0, "columns are walked two voxels at a time");
+    const uint4 tgt = M.tgt;
+    const uint32_t pitch = tgt.x;
+    const uint4 fb = M.fast;
+    const float hv = a.half_minus_off;
+    const uint64_t magic = f2pack(8388608.0f, 8388608.0f);
+    if (M.flags.z) {
+        // untilted: u, w and 1/w are column invariants, v = fma(py, Qv, Rv)
+        const float rw = __frcp_rn(Cw);
+        const float Qv = __fmul_rn(M.cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
+        const uint64_t Q2 = f2pack(Qv, Qv), R2 = f2pack(Rv, Rv);
+        const uint32_t du = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x);
+        if (M.flags.w) {
+            // dv = bits(fadd_rz(yv, 2^23)) - fb.z is in [0, rows) for every voxel, so the
+            // index dv * pitch + du + off is bits * pitch + (du + off - fb.z * pitch) mod 2^32
+            const uint32_t K = du + tgt.y - fb.z * pitch;
+#pragma unroll
+            for (int k = 0; k < LEN; k += 2) {
+                uint32_t b0, b1;
+                u2unpack(addrz2(fma2(py2[k >> 1], Q2, R2), magic), b0, b1);
+                f(std::true_type{}, k, true, b0 * pitch + K);
+                f(std::true_type{}, k + 1, true, b1 * pitch + K);
+            }
+            return 2;
+        }
+        const bool in_u = du < fb.y;
+        if (!__any_sync(0xffffffffu, in_u)) return 0;
+        const uint32_t K = du + tgt.y;
+#pragma unroll
+        for (int k = 0; k < LEN; k += 2) {
+            uint32_t b0, b1;
+            u2unpack(addrz2(fma2(py2[k >> 1], Q2, R2), magic), b0, b1);
+            const uint32_t dv0 = b0 - fb.z, dv1 = b1 - fb.z;
+            f(std::false_type{}, k, in_u && (dv0 < fb.w), dv0 * pitch + K);
+            f(std::false_type{}, k + 1, in_u && (dv1 < fb.w), dv1 * pitch + K);
+        }
+        return 1;
+    }
+    Packed kp;
+    kp.magic = magic;
+    kp.cuy = f2pack(M.cu.y, M.cu.y);
+    kp.cvy = f2pack(M.cv.y, M.cv.y);
+    kp.cwy = f2pack(M.cw.y, M.cw.y);
+    kp.Cu = f2pack(Cu, Cu);
+    kp.Cv = f2pack(Cv, Cv);
+    kp.Cw = f2pack(Cw, Cw);
+    kp.half = f2pack(0.5f, 0.5f);
+    kp.hv = f2pack(hv, hv);
+    if (M.flags.w) {
+        const uint32_t Ku = tgt.y - fb.z * pitch - fb.x;
+#pragma unroll
+        for (int k = 0; k < LEN; k += 2) {
+            uint64_t bu, bv;
+            tilted_pair(py2[k >> 1], kp, bu, bv);
+            uint32_t bu0, bu1, bv0, bv1;
+            u2unpack(bu, bu0, bu1);
+            u2unpack(bv, bv0, bv1);
+            f(std::true_type{}, k, true, bv0 * pitch + bu0 + Ku);
+            f(std::true_type{}, k + 1, true, bv1 * pitch + bu1 + Ku);
+        }
+        return 2;
+    }
+#pragma unroll
+    for (int k = 0; k < LEN; k += 2) {
+        uint64_t bu, bv;
+        tilted_pair(py2[k >> 1], kp, bu, bv);
+        uint32_t bu0, bu1, bv0, bv1;
+        u2unpack(bu, bu0, bu1);
+        u2unpack(bv, bv0, bv1);
+        const uint32_t du0 = bu0 - fb.x, du1 = bu1 - fb.x, dv0 = bv0 - fb.z, dv1 = bv1 - fb.z;
+        f(std::false_type{}, k, (du0 < fb.y) && (dv0 < fb.w), dv0 * pitch + du0 + tgt.y);
+        f(std::false_type{}, k + 1, (du1 < fb.y) && (dv1 < fb.w), dv1 * pitch + du1 + tgt.y);
+    }
+    return 1;
+}
+
+// Column walker.  For the voxel column (ax, az) and y-positions py[0..LEN) (in pairs
+// py2[m] = {py[2m], py[2m + 1]}), calls
 // f(inside, k, in, idx) with idx the target index of ProjMeta.  Untilted projections
 // (flags.z) hoist u, w and 1/w out of the column; the others evaluate the full
 // contract per voxel.  In the FAST contract a brick whose footprint lies inside the
 // viewport (flags.w) skips the bounds tests: `inside` is then std::true_type and
 // `in` is true for every voxel.  Returns 0, without calling f, when no column of the
 // warp meets the projection's u range; 2 when the inside path ran; 1 otherwise.
-template <int ARITH, int LEN, typename F>
-__device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &a, int ax, int az,
-                                           const float (&py)[LEN], F &&f)
+template <int ARITH, int LEN, typename PY, typename F>
+__device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &a, int ax, int az, const PY &py2,
+                                           F &&f)
 {
     const float4 cu = M.cu, cv = M.cv, cw = M.cw;
     const uint4 tgt = M.tgt;
@@ -334,7 +501,7 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
     const float pz = pos<ARITH>(az, a.voxel[2], a.origin[2]);
     const uint32_t pitch = tgt.x;
     if (ARITH == kFast)
-        return walk_fast<LEN>(M, a, col_fast(cu, px, pz), col_fast(cv, px, pz), col_fast(cw, px, pz), py, f);
+        return walk_fast<LEN>(M, a, col_fast(cu, px, pz), col_fast(cv, px, pz), col_fast(cw, px, pz), py2, f);
     {  // STRICT
         const int4 rc = M.rect;
         const float off = a.row_off_f;
@@ -351,16 +518,17 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
             const float Pv = __fmul_rn(cv.x, px), Rv = __fmul_rn(cv.z, pz);
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float nv = __fadd_rn(__fadd_rn(__fadd_rn(Pv, __fmul_rn(cv.y, py[k])), Rv), cv.w);
+                const float nv = __fadd_rn(__fadd_rn(__fadd_rn(Pv, __fmul_rn(cv.y, ypos(py2, k))), Rv), cv.w);
                 const uint32_t dv = (uint32_t)(__float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off))) - rc.z);
                 f(std::false_type{}, k, in_u && (dv < (uint32_t)rc.w), dv * pitch + K);
             }
         } else {
 #pragma unroll
             for (int k = 0; k < LEN; ++k) {
-                const float nu = num_strict(cu, px, py[k], pz);
-                const float nv = num_strict(cv, px, py[k], pz);
-                const float nw = num_strict(cw, px, py[k], pz);
+                const float py = ypos(py2, k);
+                const float nu = num_strict(cu, px, py, pz);
+                const float nv = num_strict(cv, px, py, pz);
+                const float nw = num_strict(cw, px, py, pz);
                 const uint32_t du = (uint32_t)(__float2int_rz(roundf(__fdiv_rn(nu, nw))) - rc.x);
                 const uint32_t dv = (uint32_t)(__float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off))) - rc.z);
                 f(std::false_type{}, k, (du < (uint32_t)rc.y) && (dv < (uint32_t)rc.w), dv * pitch + du + tgt.y);
@@ -639,11 +807,15 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
 
     // the column's y positions are the same for every thread: kept in shared memory
     // (read as broadcasts), which leaves the registers to the sums and the gathers in flight
-    __shared__ __align__(16) float py[CB];
+    __shared__ __align__(16) uint64_t py[CB / 2];  // in pairs {py[2m], py[2m + 1]}
     float s[CB];
     uint32_t n2[CB / 2];  // in-bounds counts, two 16-bit halves per word (k even: low, odd: high)
     uint32_t n_inside = 0;  // projections walked on the inside path: every voxel of the column counted
-    if (threadIdx.x < CB) py[threadIdx.x] = pos<ARITH>(a.vmin[1] + y0 + (int)threadIdx.x, a.voxel[1], a.origin[1]);
+    if (threadIdx.x < CB / 2) {
+        const int k = 2 * (int)threadIdx.x;
+        py[threadIdx.x] = f2pack(pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]),
+                                 pos<ARITH>(a.vmin[1] + y0 + k + 1, a.voxel[1], a.origin[1]));
+    }
 #pragma unroll
     for (int k = 0; k < CB; ++k) s[k] = 0.0f;
 #pragma unroll
