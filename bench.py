@@ -86,7 +86,7 @@ NOMINAL_FP32_LANES = 148 * 128
 # DRAM bytes (read + write) per voxel per launch, from one ncu capture of each kernel on the
 # c2 geometry's central 256-layer slab (FAST contract, FP32 storage: 718.1 MB and 1210.0 MB
 # for 150,994,944 voxels); scaled to a launch by its voxel count for the same geometry
-MEASURED_TRAFFIC_PER_VOXEL = {"forward": 718.1e6 / 150994944, "backward": 1210.0e6 / 150994944}
+MEASURED_TRAFFIC_PER_VOXEL = {"forward": 716.1e6 / 150994944, "backward": 1219.0e6 / 150994944}
 
 
 def parse_args():
