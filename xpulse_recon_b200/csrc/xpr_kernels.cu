@@ -838,7 +838,23 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
             // an out-of-bounds pair contributes r = 0, and s + 0 == s exactly (s is never -0).
             // Raw bits first, values after: the loads of the column stay independent of
             // any conversion, so they are all in flight together in every storage type.
+            // consumed in two halves of CB / 2 gathers (each half all in flight), which keeps
+            // the registers of the gathers in flight to CB / 2
             uint32_t rb[CB];
+            auto consume = [&](int k0) {
+#pragma unroll
+                for (int k = k0; k < k0 + CB / 2; ++k) {
+                    const float r = ratio_from_bits<DT>(rb[k]);
+                    if (NANSKIP) {
+                        if (r == r) {
+                            s[k] = __fadd_rn(s[k], r);
+                            n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
+                        }
+                    } else {
+                        s[k] = __fadd_rn(s[k], r);
+                    }
+                }
+            };
             const int walked = walk_column<ARITH, CB>(M, a, ax, az, py, [&](auto inside, int k, bool in, uint32_t idx) {
                 rb[k] = 0u;
                 if (in) rb[k] = load_ratio_bits<DT>(ratio, idx);
@@ -846,21 +862,11 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
                     if (!NANSKIP && in) n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
                     if (NANSKIP && !in) rb[k] = kNaNBits<DT>;
                 }
+                if (k == CB / 2 - 1) consume(0);
             });
             if (!walked) continue;  // warp-uniform
             if (!NANSKIP && walked == 2) ++n_inside;
-#pragma unroll
-            for (int k = 0; k < CB; ++k) {
-                const float r = ratio_from_bits<DT>(rb[k]);
-                if (NANSKIP) {
-                    if (r == r) {
-                        s[k] = __fadd_rn(s[k], r);
-                        n2[k >> 1] += (k & 1) ? 0x10000u : 1u;
-                    }
-                } else {
-                    s[k] = __fadd_rn(s[k], r);
-                }
-            }
+            consume(CB / 2);
         }
         __syncthreads();
     }
