@@ -9,26 +9,29 @@
 // is bound by FP32 issue and atomic throughput, not by HBM bytes, so the
 // kernels are organised to cut atomics and redundant arithmetic:
 //
-//  * A CTA owns a brick of 32 x 8 x 32 voxels (x, y, z) for a run of
-//    projections.  The forward keeps the brick in shared memory as 22-bit
+//  * A forward CTA owns a brick of 32 x 8 x 32 voxels (x, y, z) for a run of
+//    projections (a backward CTA one of 32 x 16 x 8).  The forward keeps the brick in shared memory as 22-bit
 //    fixed point (loaded once, coalesced), projects its 8 corners per
 //    projection to bound its detector footprint, splats into a shared-memory
 //    tile of that footprint with shared atomics, and flushes the tile with one
 //    coalesced global atomic per touched pixel.  Bricks whose footprint misses
 //    the viewport are skipped; all-zero bricks are skipped.
-//  * Each thread walks one line of voxels along the axis closest to the ray
-//    (x or z, chosen per projection) with its 32 lanes across the ray, so the
-//    lanes of a warp hit distinct pixels, and consecutive voxels on the line
-//    (which mostly land on the same pixel) are summed in a register before an
-//    atomic is issued.  Integer atomics commute, so the result is bit-identical
-//    to the reference's voxel-per-work-item order.
+//  * Each thread walks vertical voxel columns (along y).  For an untilted
+//    detector a column lands in one detector column with one 1/w, so a voxel
+//    costs one packed FMA and one round-toward-zero add for its row, one
+//    multiply-add for its tile index, a quarter of a 128-bit shared load for
+//    its value and one shared atomic.  The 32 lanes of a warp run across the ray
+//    (x or z, chosen per projection), so they mostly hit distinct pixels.
+//    Integer atomics commute, so the result is bit-identical to the reference's
+//    voxel-per-work-item order.
 //  * The backward keeps each voxel's running sum and count in registers and
 //    visits projections in the reference's order, so the floating-point sum is
 //    the reference's sum; detector gathers go through the read-only L1 path,
 //    which the brick's small footprint keeps resident.
-//  * Along a line the per-row projective numerators are affine; the line
-//    invariant part is computed once per line (see xpr_math.cuh for the exact
-//    operation contracts).
+//  * Along a column the projective numerators are affine in y; the column
+//    invariant part is computed once per column, and in the forward the lane
+//    coordinate's share of it once per projection (see xpr_math.cuh for the
+//    exact operation contracts).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
