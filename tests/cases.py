@@ -20,6 +20,9 @@ CASES = {
                          mod_rpy=[[1.0, -0.5, 0.8], [0.0, 0.3, -1.2], [-1.5, 0.9, 0.2]]),
     "helical": dict(dwidth=40, dheight=24, projections=30, sit=3, heli_offset=0.05),
     "shortscan": dict(dwidth=48, dheight=48, projections=30, sit=3, angle=200.0),
+    # wide cone (source close to the object): near-source bricks project large enough that
+    # the forward splats them with global atomics instead of a shared-memory tile
+    "widecone": dict(dwidth=96, dheight=40, projections=24, sit=3, so=2.0, sd=4.0, rx=0.5, sy=1.0),
     "anglelist": dict(dwidth=32, dheight=32, projections=12, sit=2,
                       angle_list=[0.0, 7.5, 31.0, 44.0, 90.0, 95.5, 180.0, 181.0, 250.0, 271.0, 300.0, 359.0]),
 }

@@ -117,7 +117,7 @@ def test_forward_backward_with_angle_lists(ctx, arith):
 
 
 @pytest.mark.parametrize("arith", [O.STRICT, O.FAST])
-@pytest.mark.parametrize("name", ["plain48", "offsets64", "modules3_rpy", "helical"])
+@pytest.mark.parametrize("name", ["plain48", "offsets64", "modules3_rpy", "helical", "widecone"])
 def test_backward_bit_exact(ctx, name, arith):
     c = make_case(name, sit=2, seed=15)
     ratio = ratio_from(c, oracle_forward(c, arith))
