@@ -95,14 +95,18 @@ def parse_args():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--arith", choices=["fast", "strict"], default="fast")
+    p.add_argument("--arith", choices=["fast", "strict"], default="strict",
+                   help="projector contract: strict = the reference kernels' IEEE results bit for bit (default)")
     p.add_argument("--storage", choices=["fp32", "bf16", "fp16"], default=None,
                    help="image / ratio storage (default: fp32; bf16 for the batched configurations)")
     p.add_argument("--config", choices=sorted(CONFIGS), default="c2")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--shard", action="store_true",
-                   help="N > 1: one reconstruction split into y-slabs over the ranks (u32 all-reduce of the "
-                        "detector sums per sub-iteration, strong scaling) instead of one per rank")
+                   help="one reconstruction split into y-slabs over the ranks (the default for N > 1): the "
+                        "u32 detector sums of the rows where neighbouring slabs' footprints overlap are "
+                        "exchanged each sub-iteration (strong scaling)")
+    p.add_argument("--replicas", action="store_true",
+                   help="N > 1: an independent reconstruction per rank instead (weak scaling, no exchange)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     return p.parse_args()
 
@@ -266,6 +270,7 @@ class Problem:
         with torch.cuda.stream(self.stream):
             phantom = make_phantom(cfg, self.g["vx"], self.W, self.Hv, d, seed, self.y0, self.y1)
             self.images = []
+            self.raw_host = []  # the raw intensities I / I0 of each subset (for the raw end-to-end leg)
             sums = torch.zeros(self.npix, dtype=torch.int32, device=d)
             gen = torch.Generator(device=d).manual_seed(seed + 1)
             for s in range(self.S):
@@ -277,6 +282,7 @@ class Problem:
                 _lib.check(self.L.xpr_preprocess_apply(self.ctx.handle, inten.data_ptr(), out.data_ptr(), self.storage,
                                                        self.npix, 0, None, 1, self.sp), "preprocess")
                 self.images.append(out)
+                self.raw_host.append(inten.cpu())
                 del p, inten
             self.phantom_host = None
             self.phantom = phantom
@@ -345,10 +351,16 @@ class Problem:
 
 
 # ----------------------------------------------------------------------------- CPU (reference kernels)
-def cpu_reference_step_factory(cfg, seconds_target):
+REF_SAMPLE_LAYERS = 128  # the central y-slab both CPU legs time when the whole grid is too large
+
+
+def cpu_reference_step_factory(cfg, seconds_target, max_layers=REF_SAMPLE_LAYERS):
     """The reference's own OpenCL kernels (oracle/_ref, built from its sources) on the host
     cores: forward + error + backward of a y-slab of the grid against one sub-iteration's
-    72 projections.  Returns (step_fn, info)."""
+    projections -- the whole grid when it is small (c1), else the central max_layers layers
+    (the same sample for cpu_baseline and the reference arm, so that their fixed costs --
+    the error step over the whole detector -- weigh the same).  seconds_target only sets
+    how often a whole small grid is repeated.  Returns (step_fn, info)."""
     from oracle import oracle as O
     R = O.ref_lib()
     kind = "reference"
@@ -384,16 +396,15 @@ def cpu_reference_step_factory(cfg, seconds_target):
                 O.backward(vol, sums.view(np.float32), pd, L)
         return time.perf_counter() - t, n * Pc * reps
 
-    # calibrate on a few layers (one layer is dominated by fixed costs), then size the sample:
-    # a slab of the grid, or the whole grid repeated when the grid is smaller than the target
-    probe = min(8, Hv)
-    dt, pairs = run(probe)
-    layers = int(max(1, min(Hv, round(probe * seconds_target / max(dt, 1e-3)))))
+    whole = W * Hv * W * Pc <= 2e9
+    layers = Hv if whole else min(Hv, max_layers)
     reps = 1
-    if layers == Hv:
+    if whole:
         dt_full, _ = run(Hv)
         reps = int(max(1, round(seconds_target / max(dt_full, 1e-3))))
-    info = {"kind": kind, "cores": os.cpu_count(), "layers": layers, "W": W, "Pc": Pc, "reps": reps}
+    info = {"kind": kind, "cores": os.cpu_count(), "layers": layers, "W": W, "Hv": Hv, "Pc": Pc, "reps": reps}
+    if not whole and max_layers <= 8:
+        info["probe_s"], _ = run(layers)  # a timing probe of the thin slab
     return (lambda: run(layers, reps)), info
 
 
@@ -416,7 +427,15 @@ def run_reference(args, cfg, rank, world):
               "batched / served / out-of-core workload of this library (time its single-problem kernels with "
               "--config c2)" % args.config})
         return 0
-    step, info = cpu_reference_step_factory(cfg, max(1.0, min(10.0, 60.0 / max(1, args.steps + args.warmup))))
+    # the cpu_baseline sample (whole small grids once per step; else the central 128-layer slab,
+    # thinned to no fewer than 64 layers if the whole run would take over about four minutes)
+    n = max(1, args.steps + args.warmup)
+    _, probe_info = cpu_reference_step_factory(cfg, 0.0, max_layers=8)
+    layers = REF_SAMPLE_LAYERS
+    if probe_info["layers"] < probe_info["Hv"]:
+        t8 = probe_info["probe_s"]
+        layers = int(max(64, min(REF_SAMPLE_LAYERS, 8 * 240.0 / n / max(t8, 1e-3))))
+    step, info = cpu_reference_step_factory(cfg, 0.0, max_layers=layers)
     for _ in range(args.warmup):
         step()
     tot_t, tot_p = 0.0, 0
@@ -487,22 +506,36 @@ def run_ours(args, cfg, rank, world, local):
         host = prob.images[s].view(torch.uint8).cpu().numpy()  # keep alive across the copy
         C.memmove(hp, host.ctypes.data, nbytes)
         pinned.append(hp)
+    # the raw leg: intensities I / I0 (float32) go up instead, and -log runs on the device
+    raw_bytes = prob.npix * 4
+    pinned_raw = []
+    for s in range(prob.S):
+        hp = C.c_void_p()
+        _lib.check(L.xpr_alloc_pinned(prob.ctx.handle, raw_bytes, C.byref(hp)), "alloc_pinned")
+        host = prob.raw_host[s].numpy()
+        C.memmove(hp, host.ctypes.data, raw_bytes)
+        pinned_raw.append(hp)
     res_host = C.c_void_p()
     _lib.check(L.xpr_alloc_pinned(prob.ctx.handle, 8, C.byref(res_host)), "alloc_pinned")
     dbuf = [torch.empty_like(prob.images[0]) for _ in range(2)]
+    rbuf = [torch.empty(prob.npix, dtype=torch.float32, device=prob.device) for _ in range(2)]
     copy_stream = torch.cuda.Stream(device=prob.device)
     cs = C.c_void_p(copy_stream.cuda_stream)
     up_done = [torch.cuda.Event() for _ in range(2)]
     used = [torch.cuda.Event() for _ in range(2)]
 
-    def e2e_steps(n, timed):
+    def e2e_steps(n, timed, raw=False):
+        """n sub-iterations with each subset's images uploaded from page-locked host memory
+        (double-buffered on a copy stream) and the residual read back; raw: the uploads are
+        the raw intensities and the -log preprocessing runs on the device in the step."""
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        src, dst, size = (pinned_raw, rbuf, raw_bytes) if raw else (pinned, dbuf, nbytes)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         start.record(prob.stream)
         s0 = prob.sit_next
-        _lib.check(L.xpr_upload(prob.ctx.handle, dbuf[0].data_ptr(), pinned[s0], nbytes, cs), "upload")
+        _lib.check(L.xpr_upload(prob.ctx.handle, dst[0].data_ptr(), src[s0], size, cs), "upload")
         up_done[0].record(copy_stream)
         for k in range(n):
             b = k % 2
@@ -511,9 +544,12 @@ def run_ours(args, cfg, rank, world, local):
                 if k >= 1:
                     copy_stream.wait_event(used[nb])
                 nxt = (prob.sit_next + 1) % prob.S
-                _lib.check(L.xpr_upload(prob.ctx.handle, dbuf[nb].data_ptr(), pinned[nxt], nbytes, cs), "upload")
+                _lib.check(L.xpr_upload(prob.ctx.handle, dst[nb].data_ptr(), src[nxt], size, cs), "upload")
                 up_done[nb].record(copy_stream)
             prob.stream.wait_event(up_done[b])
+            if raw:
+                _lib.check(L.xpr_preprocess_apply(prob.ctx.handle, rbuf[b].data_ptr(), dbuf[b].data_ptr(),
+                                                  prob.storage, prob.npix, 0, None, 1, prob.sp), "preprocess")
             prob.subiteration(images=dbuf[b])
             used[b].record(prob.stream)
             _lib.check(L.xpr_download(prob.ctx.handle, res_host, prob.residual.data_ptr(), 8, prob.sp), "download")
@@ -528,7 +564,14 @@ def run_ours(args, cfg, rank, world, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = pairs_step * K * world / (e2e_ms / 1000.0) / 1e9
-    for hp in pinned:
+    e2e_steps(min(2, K), False, raw=True)
+    raw_ms = e2e_steps(K, True, raw=True)
+    if dist:
+        t = torch.tensor([raw_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        raw_ms = float(t.item())
+    e2e_raw_value = pairs_step * K * world / (raw_ms / 1000.0) / 1e9
+    for hp in pinned + pinned_raw:
         L.xpr_free_pinned(prob.ctx.handle, hp)
     L.xpr_free_pinned(prob.ctx.handle, res_host)
 
@@ -564,7 +607,13 @@ def run_ours(args, cfg, rank, world, local):
                    "projections": prob.P, "sit": prob.S, "per_subiteration": prob.Pc, "arith": args.arith,
                    "storage": args.storage, "l2": "inputs larger than L2 (%.2f GB volume, %.0f MB subset)"
                    % (4 * prob.nvox / 1e9, isz * prob.npix / 1e6), "parallelism": "independent volume per rank"},
-        "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": 8},
+        "e2e": {"value": e2e_value, "unit": "GUPS", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": 8,
+                "what": "steady-state sub-iterations: each step uploads its subset's preprocessed images from "
+                        "page-locked host memory and reads the residual back"},
+        "e2e_raw": {"value": e2e_raw_value, "unit": "GUPS", "h2d_bytes_per_step": raw_bytes,
+                    "d2h_bytes_per_step": 8,
+                    "what": "as e2e, but each step uploads the raw intensities I / I0 and runs the -log "
+                            "preprocessing on the device inside the step"},
         "gpu_launches": 3 * K,
         "kernels_ms": {"forward": f_ms, "error": statistics.mean(err), "backward": b_ms},
         "kernel_gups": {"forward": pairs_step / (f_ms / 1000.0) / 1e9, "backward": pairs_step / (b_ms / 1000.0) / 1e9},
@@ -909,8 +958,10 @@ def run_serving(args, cfg, rank, world, local):
 # ----------------------------------------------------------------------------- slab-sharded
 def run_sharded(args, cfg, rank, world, local):
     """One c2 reconstruction split into y-slabs over the ranks (xpulse_recon_b200.shard):
-    per sub-iteration a slab forward, an NCCL all-reduce of the u32 detector sums, the
-    error and a slab backward.  Total work is fixed as N grows (strong scaling)."""
+    per sub-iteration a slab forward into the detector rows the slab reaches, a
+    point-to-point NCCL exchange of the u32 sums over the rows shared with other ranks,
+    the error on the rank's rows and a slab backward.  Total work is fixed as N grows
+    (strong scaling)."""
     import datetime
 
     import torch
@@ -918,7 +969,8 @@ def run_sharded(args, cfg, rank, world, local):
     from xpulse_recon_b200.shard import GpuOps, SlabReconstruction
     torch.cuda.set_device(local)
     if world > 1:
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist.barrier()  # every rank takes part in the communicator's first call
     args.storage = args.storage or "fp32"
     prob = Problem(cfg, args.arith, args.storage, local, cfg["seed"])  # the same measured data on every rank
     images = torch.cat(prob.images)
@@ -932,6 +984,7 @@ def run_sharded(args, cfg, rank, world, local):
     for k in range(Wm + 1):  # step 0 has no forward: warm-up starts with it
         r.step(k)
     torch.cuda.synchronize()
+    sent0 = r.exchanged_bytes
     if world > 1:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -954,9 +1007,10 @@ def run_sharded(args, cfg, rank, world, local):
             "n_gpus": world, "steps": K, "warmup": Wm + 1, "ms_per_step": ms / K, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.config + ": " + cfg["desc"], "parallelism": "y-slab sharding, %d ranks, "
-                       "u32 all-reduce of the detector sums" % world, "arith": args.arith, "storage": args.storage,
-                       "l2": "inputs larger than L2"},
-            "exchange_bytes_per_step": 4 * prob.npix if world > 1 else 0, "gpu_launches": 3 * K,
+                       "u32 sums of the shared detector rows exchanged point to point" % world,
+                       "arith": args.arith, "storage": args.storage, "l2": "inputs larger than L2",
+                       "row_window": [r.r0, r.r1]},
+            "exchange_bytes_per_step": (r.exchanged_bytes - sent0) / K, "gpu_launches": 3 * K,
             "clocks": clk}
     if rank == 0:
         emit(line)
@@ -1063,7 +1117,7 @@ def main():
         return run_batched(args, cfg, rank, world, local)
     if cfg.get("serve"):
         return run_serving(args, cfg, rank, world, local)
-    if args.shard:
+    if args.shard or (world > 1 and not args.replicas):
         return run_sharded(args, cfg, rank, world, local)
     if cfg.get("outofcore"):
         return run_outofcore(args, cfg, rank, world, local)

@@ -37,7 +37,8 @@ enum xpr_status {
     XPR_ERR_INVALID = 1,     /* bad argument */
     XPR_ERR_CUDA = 2,        /* CUDA runtime error */
     XPR_ERR_OOM = 3,         /* device or pinned allocation failed */
-    XPR_ERR_CAP = 4,         /* request exceeds the context's device-memory cap */
+    XPR_ERR_CAP = 4,         /* request exceeds the context's device-memory cap, or the capacity of a
+                                fixed-size scratch (xpr_subiteration_static) */
     XPR_ERR_IO = 5,          /* file read / write failure */
     XPR_ERR_PARAM = 6,       /* malformed or inconsistent parameters (JSON, geometry) */
     XPR_ERR_UNSUPPORTED = 7  /* valid request this build does not implement */
@@ -180,7 +181,7 @@ uint64_t xpr_subiteration_static_capacity(void);
 typedef struct xpr_batch_problem {
     float *vol;                   /* device, vwidth * vheight * vwidth floats (x fastest, then z, then y) */
     const void *images;           /* device, sit * per_subset preprocessed images of det_w * det_h in the batch's
-                                     storage type, subset-major: subset s holds acquisitions s, s + sit, ... */
+                                     image storage type, subset-major: subset s holds acquisitions s, s + sit, ... */
     const xpr_projdata *projdata; /* device, sit * per_subset * modules entries in the same order */
     uint32_t det_w, det_h;
     uint32_t per_subset;          /* projections per sub-iteration: floor(projections / sit) */
@@ -196,13 +197,16 @@ typedef struct xpr_batch_problem {
 
 typedef struct xpr_batch_opts {
     int32_t arith;                /* xpr_arith */
-    int32_t storage;              /* xpr_dtype of the images and of the ratio scratch */
+    int32_t storage;              /* xpr_dtype of the ratio scratch, and of the images unless
+                                     image_storage_set */
     int32_t init_volume;          /* each run first sets every volume to 1.0 (reconstruction_n.hpp:59) */
     int32_t use_graph;            /* capture the whole run into one CUDA graph at the first run, replay after */
     int32_t autotune;             /* time the schedule candidates once (per batch shape, cached) */
     int32_t fwd_splits;           /* 0: automatic or tuned; else projection runs per forward brick */
     int32_t bwd_column;           /* 0: automatic or tuned; else 8 or 16 layers per backward voxel column */
     int32_t ctas_per_sm;          /* 0: the occupancy limit */
+    int32_t image_storage_set;    /* 0: the measured images are stored in `storage` too */
+    int32_t image_storage;        /* else their xpr_dtype, e.g. FP16 images with a BF16 ratio */
 } xpr_batch_opts;
 
 typedef struct xpr_batch xpr_batch;
@@ -238,9 +242,12 @@ int xpr_batch_destroy(xpr_batch *b);
  * reference. */
 typedef struct xpr_serve_opts {
     int32_t arith;                /* xpr_arith for every request */
-    int32_t storage;              /* xpr_dtype of the images and ratios of every request */
+    int32_t storage;              /* xpr_dtype of the ratios of every request, and of its images unless
+                                     image_storage_set */
     uint64_t mem_budget;          /* device bytes for resident requests; 0: 90% of the free memory */
     uint32_t max_active;          /* requests resident at once; 0: no limit */
+    int32_t image_storage_set;    /* 0: images stored in `storage` */
+    int32_t image_storage;        /* else the xpr_dtype of the preprocessed images */
 } xpr_serve_opts;
 
 enum xpr_request_state { XPR_REQ_QUEUED = 0, XPR_REQ_ACTIVE = 1, XPR_REQ_DONE = 2, XPR_REQ_FAILED = 3 };

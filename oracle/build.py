@@ -6,7 +6,14 @@ Two libraries are produced:
 * ``oracle/_build/libxpr_oracle.so`` -- the C restatement in ``xpr_oracle.c``.
 * ``oracle/_ref/libxpr_ref.so`` -- the reference's own OpenCL kernel sources
   (``src/reconstruction/gpu/kernels/Kernel*.cl`` of ebarjou/xpulse_recon),
-  compiled for the CPU through ``ref_shim.hpp``.  The sources are read where
+  compiled for the CPU through ``ref_shim.hpp``.
+* ``oracle/_ref/libxpr_ref_relaxed.so`` -- the same generated sources compiled with
+  relaxed floating point (``-ffast-math -mfma``: contraction into fma, reassociation,
+  reciprocal division, no signed zeros), a CPU stand-in for the reference's own build
+  flags (src/reconstruction/gpu/kernel.hpp:26-30 builds every program with
+  ``-cl-fast-relaxed-math -cl-mad-enable -cl-no-signed-zeros
+  -cl-unsafe-math-optimizations -cl-finite-math-only``).  It measures how far a legitimate relaxed compilation of the
+  reference lands from its IEEE interpretation.  The sources are read where
   they lie in the reference checkout; only generated, git-ignored files are
   written under ``oracle/_ref/``.  The pre-pass is textual and mechanical:
 
@@ -21,7 +28,9 @@ Two libraries are produced:
      NaN / out-of-range values; GPUs saturate and map NaN to 0).
 
 The reference checkout is only needed to (re)generate ``oracle/_ref``; where it
-is absent the prebuilt library is used as is.
+is absent the prebuilt libraries are used as they are.  Its location is the
+``XPR_REFERENCE`` environment variable, else a ``reference`` directory beside the
+repository checkout.
 """
 from __future__ import annotations
 
@@ -35,10 +44,12 @@ BUILD_DIR = os.path.join(HERE, "_build")
 REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(BUILD_DIR, "libxpr_oracle.so")
 REF_SO = os.path.join(REF_DIR, "libxpr_ref.so")
-DEFAULT_REFERENCE = "/root/reference"
+REF_RELAXED_SO = os.path.join(REF_DIR, "libxpr_ref_relaxed.so")
+DEFAULT_REFERENCE = os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 KERNEL_DIR = os.path.join("src", "reconstruction", "gpu", "kernels")
 
 CFLAGS = ["-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC"]
+RELAXED_CFLAGS = ["-O2", "-fopenmp", "-ffast-math", "-mfma", "-mavx2", "-fPIC"]
 
 # kernel name -> launcher (the reference's argument lists, constants.cl:30-88)
 LAUNCHERS = {
@@ -179,7 +190,8 @@ def build_ref(reference_root: str | None = None, force: bool = False) -> str | N
     shim = os.path.join(HERE, "ref_shim.hpp")
     cl_files = [os.path.join(kdir, n + ".cl") for n in LAUNCHERS] + [
         os.path.join(kdir, "utils.cl"), os.path.join(kdir, "constants.cl")]
-    if not force and _newer(REF_SO, cl_files + [shim, __file__, os.path.join(HERE, "xpr_oracle.c")]):
+    deps = cl_files + [shim, __file__, os.path.join(HERE, "xpr_oracle.c")]
+    if not force and _newer(REF_SO, deps) and _newer(REF_RELAXED_SO, deps):
         return REF_SO
     objs = []
     for name, launcher in LAUNCHERS.items():
@@ -207,6 +219,14 @@ def build_ref(reference_root: str | None = None, force: bool = False) -> str | N
     _run(["gcc", "-std=c11", "-c", *CFLAGS, "-o", orc_obj, os.path.join(HERE, "xpr_oracle.c")])
     objs.append(orc_obj)
     _run(["g++", "-shared", "-fopenmp", "-o", REF_SO, *objs, "-lm"])
+    # the relaxed-math build of the same kernel sources (exp / log stay the oracle's)
+    robjs = []
+    for name in LAUNCHERS:
+        cpp = os.path.join(REF_DIR, name + ".cpp")
+        obj = os.path.join(REF_DIR, name + ".relaxed.o")
+        _run(["g++", "-std=c++17", "-c", *RELAXED_CFLAGS, "-w", "-o", obj, cpp])
+        robjs.append(obj)
+    _run(["g++", "-shared", "-fopenmp", "-o", REF_RELAXED_SO, *robjs, common[:-4] + ".o", orc_obj, "-lm"])
     return REF_SO
 
 

@@ -21,6 +21,7 @@ FIXED_ONE = 1 << 22
 
 _oracle = None
 _ref = None
+_ref_relaxed = None
 
 f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
@@ -114,14 +115,18 @@ def lib():
     return _oracle
 
 
-def ref_lib():
-    """The reference's own kernels compiled for the CPU, or None if unavailable."""
-    global _ref
-    if _ref is None:
-        path = _build.REF_SO if os.path.exists(_build.REF_SO) else _build.build_ref()
-        if path is None or not os.path.exists(path):
+def ref_lib(relaxed: bool = False):
+    """The reference's own kernels compiled for the CPU (IEEE single precision), or with
+    relaxed=True the same sources under relaxed floating point; None if unavailable."""
+    global _ref, _ref_relaxed
+    cached = _ref_relaxed if relaxed else _ref
+    if cached is None:
+        target = _build.REF_RELAXED_SO if relaxed else _build.REF_SO
+        if not os.path.exists(target):
+            _build.build_ref()
+        if not os.path.exists(target):
             return None
-        R = C.CDLL(path)
+        R = C.CDLL(target)
         u32x = C.POINTER(C.c_uint32)
         f4 = C.POINTER(C.c_float)
         i32x = C.POINTER(C.c_int32)
@@ -132,8 +137,12 @@ def ref_lib():
                                     C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64]
         R.refk_backwardh.argtypes = [f32p, f32p, f32p, u16p, u16p, C.c_uint32, C.c_uint32, f4, C.c_float,
                                      C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64]
-        _ref = R
-    return _ref
+        if relaxed:
+            _ref_relaxed = R
+        else:
+            _ref = R
+        cached = R
+    return cached
 
 
 # --------------------------------------------------------------------------- helpers
@@ -228,8 +237,8 @@ def _c_arr(ctype, vals):
     return (ctype * len(vals))(*vals)
 
 
-def ref_forward(vol, sums, pd, det_w, det_h, origin, n_angles, modules, vmin, vmax, line_offset, voxel, pad=True):
-    R = ref_lib()
+def ref_forward(vol, sums, pd, det_w, det_h, origin, n_angles, modules, vmin, vmax, line_offset, voxel, pad=True, relaxed=False):
+    R = ref_lib(relaxed)
     n = int(np.prod(np.subtract(vmax, vmin)))
     R.refk_forward(vol, sums, pd, _c_arr(C.c_uint32, [det_w, det_h, det_w, 1]),
                    _c_arr(C.c_float, [*origin, 0.0]), n_angles, modules,
@@ -238,8 +247,8 @@ def ref_forward(vol, sums, pd, det_w, det_h, origin, n_angles, modules, vmin, vm
                    ndrange(n) if pad else n)
 
 
-def ref_backward(vol, ratio, pd, det_w, det_h, origin, n_angles, modules, vmin, vmax, line_offset, voxel, pad=True):
-    R = ref_lib()
+def ref_backward(vol, ratio, pd, det_w, det_h, origin, n_angles, modules, vmin, vmax, line_offset, voxel, pad=True, relaxed=False):
+    R = ref_lib(relaxed)
     n = int(np.prod(np.subtract(vmax, vmin)))
     R.refk_backward(vol, ratio, pd, _c_arr(C.c_uint32, [det_w, det_h, det_w, 1]),
                     _c_arr(C.c_float, [*origin, 0.0]), n_angles, modules,
@@ -248,8 +257,8 @@ def ref_backward(vol, ratio, pd, det_w, det_h, origin, n_angles, modules, vmin, 
                     ndrange(n) if pad else n)
 
 
-def ref_error(images, sums, det_w, det_h, weight):
-    R = ref_lib()
+def ref_error(images, sums, det_w, det_h, weight, relaxed=False):
+    R = ref_lib(relaxed)
     R.refk_error(images, sums, _c_arr(C.c_uint32, [det_w, det_h, det_w, 1]), sums.size, weight, ndrange(sums.size))
 
 
@@ -286,3 +295,59 @@ def recon_naive_f64(gp: GeomParams, rp: ReconParams, raw: np.ndarray, mlog: bool
     vol = np.zeros(int(go.vwidth) * int(go.vheight) * int(go.vwidth), np.float64)
     assert lib().orc64_recon_naive(C.byref(gp), C.byref(rp), imgs, vol) == 0
     return vol
+
+
+# ----------------------------------------------------------------------------- naive loop over a kernel set
+def recon_loop(kernels, pd_all, go, P, S, M, imgs, Wd, Hd, it, weight, weight_factor, seed, box=None,
+               arith=STRICT, pad=False):
+    """The naive reconstruction of reconstruction_n.hpp:27-88 as a host loop over one
+    kernel set: kernels = "ref" runs the reference's own Forward / Error / Backward
+    (oracle/_ref, its OpenCL sources compiled for the CPU; IEEE single precision, the
+    STRICT contract by construction), "ref_relaxed" the same sources under relaxed
+    floating point (the reference's -cl-fast-relaxed-math, emulated), "oracle" the C
+    restatement in contract `arith`.
+
+    Volume 1.0 (:59), sums FIXED_ONE before the first sub-iteration (:60), which skips
+    the forward (:70); per sub-iteration the origin is jittered by three
+    uniform_real_distribution<float>(0, vx) draws of std::mt19937(seed)
+    (reconstruction.hpp:268-272), the error is written over the sums (KernelError.cl)
+    and the sums are zeroed after the backward; weight *= weight_factor after each main
+    iteration (:80).  imgs: preprocessed float32[P, Hd, Wd] in acquisition order;
+    sub-iteration s uses acquisitions s, s + S, ... (geometry.hpp:306-327).  box =
+    (vmin, vmax) reconstructs that part of the grid only (the kernels' volume box);
+    pad launches the reference's NDRange padding work-items (kernel.hpp:73-81).
+    Returns the box's volume, float32[n]."""
+    W, Hv = int(go.vwidth), int(go.vheight)
+    vmin, vmax = ((0, 0, 0), (W, Hv, W)) if box is None else box
+    n = int(np.prod(np.subtract(vmax, vmin)))
+    Pc = P // S
+    vol = np.ones(ndrange(n) if pad else n, np.float32)
+    sums = np.full(Pc * Wd * Hd, FIXED_ONE, np.uint32)
+    g = MT()
+    lib().orc_mt_seed(C.byref(g), int(seed))
+    w = np.float32(weight)
+    imgs = np.asarray(imgs, np.float32).reshape(P, Hd, Wd)
+    for mit in range(it):
+        for s in range(S):
+            origin = [float(np.float32(go.orig[i]) + np.float32(lib().orc_uniform_float(C.byref(g), 0.0, go.vx)))
+                      for i in range(3)]
+            pd = np.ascontiguousarray(subset_projdata(pd_all, P, S, M, s, Pc), np.float32)
+            sub = np.ascontiguousarray(imgs[[s + k * S for k in range(Pc)]]).ravel()
+            if kernels in ("ref", "ref_relaxed"):
+                rx = kernels == "ref_relaxed"
+                if mit > 0 or s > 0:
+                    ref_forward(vol, sums, pd, Wd, Hd, origin, Pc, M, vmin, vmax, (0, Hd), [go.vx] * 3, pad=pad,
+                                relaxed=rx)
+                ref_error(sub, sums, Wd, Hd, float(w), relaxed=rx)
+                ref_backward(vol, sums.view(np.float32), pd, Wd, Hd, origin, Pc, M, vmin, vmax, (0, Hd),
+                             [go.vx] * 3, pad=pad, relaxed=rx)
+            else:
+                L, keep = make_launch(vmin, vmax, origin, [go.vx] * 3, Wd, Hd, 0, Pc, M, arith=arith,
+                                      compat_pad=int(pad))
+                if mit > 0 or s > 0:
+                    forward(vol, sums, pd, L)
+                error(sub, sums, float(w))
+                backward(vol, sums.view(np.float32), pd, L)
+            sums[:] = 0
+        w = np.float32(w * np.float32(weight_factor))
+    return vol[:n].copy()

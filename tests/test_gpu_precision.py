@@ -14,9 +14,15 @@ multiplicative update drives a few hundred of their voxels to 1e12 in either pre
 storage precision (it is reported as rel_rmse_all).  The voxels no projection reaches
 are NaN in both, by the algorithm's 0/0.
 
-Tolerances (written here, measured on B200): FP32 <= 2e-3, FP16 <= 2e-3,
-BF16 <= 5e-3 relative RMSE.  Setting XPR_PRECISION_REPORT=<path> appends one JSON
-line per (workload, storage) with the measured value."""
+Storage forms (ratio / measured images): fp32, fp16, bf16 = BF16 ratio with FP16
+images (the BF16 form of the batched and served paths), bf16_fp32img = BF16 ratio with
+FP32 images, bf16_all = BF16 ratio and BF16 images.  Tolerance (written here): 1e-3
+relative RMSE for every form but bf16_all, the north star's bound.  bf16_all is a
+known miss (measured 1.6e-3 - 2.3e-3 on B200): a BF16 measured value carries a 2^-9
+relative error, which enters the log-ratio as an absolute error of the same size; it
+is kept as an xfail so that the miss stays visible.  Setting
+XPR_PRECISION_REPORT=<path> appends one JSON line per (workload, storage) with the
+measured values (region and all voxels)."""
 import ctypes as C
 import json
 import os
@@ -32,7 +38,10 @@ from xpulse_recon_b200.projector import Context, Reconstruction, geometry  # noq
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp32": 2e-3, "fp16": 2e-3, "bf16": 5e-3}
+TOL = 1e-3
+# form: (ratio storage, image storage)
+FORMS = {"fp32": ("fp32", "fp32"), "fp16": ("fp16", "fp16"), "bf16": ("bf16", "fp16"),
+         "bf16_fp32img": ("bf16", "fp32"), "bf16_all": ("bf16", "bf16")}
 
 # name: (geometry, it, sit, ellipsoids, phantom fraction of the grid, seed)
 WORKLOADS = {
@@ -97,9 +106,11 @@ def _projections(ctx, vol, pd_all, g, det, rng, i0=1e5, jitters=4, modules=1):
     return (np.maximum(counts, 1) / i0).astype(np.float32).reshape(P_img, Hd, Wd)
 
 
-def _product(raw, geom, it, sit, storage):
-    cfg = {"recon": {"method": "naive", "it": it, "sit": sit, "seed": 5, "arith": "fast", "geometry": "fp64",
-                     "storage": storage, "mlog": True, "weight": 1.0, "weight_factor": 0.9},
+def _product(raw, geom, it, sit, form):
+    storage, image_storage = FORMS[form]
+    cfg = {"recon": {"method": "naive", "it": it, "sit": sit, "seed": 5, "arith": "strict", "geometry": "fp64",
+                     "storage": storage, "image_storage": image_storage, "mlog": True, "weight": 1.0,
+                     "weight_factor": 0.9},
            "geometry": {"so": 100.0, "sd": 1000.0, "angle": 360.0},
            "detector": {"px": 0.1, "rx": geom.get("rx", 0.0), "sx": geom.get("sx", 0.0), "sy": geom.get("sy", 0.0)}}
     if "mod_rpy" in geom:
@@ -159,7 +170,9 @@ def _workload(name):
     return _cache[name]
 
 
-@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16", "bf16_fp32img", pytest.param(
+    "bf16_all", marks=pytest.mark.xfail(strict=True, reason="BF16 measured images: 1.6e-3 - 2.3e-3 relative RMSE, "
+                                                         "above the 1e-3 bound"))])
 @pytest.mark.parametrize("name", sorted(WORKLOADS))
 def test_relative_rmse_against_fp64_oracle(name, storage):
     geom, it, sit = WORKLOADS[name][:3]
@@ -175,8 +188,9 @@ def test_relative_rmse_against_fp64_oracle(name, storage):
     report = os.environ.get("XPR_PRECISION_REPORT")
     if report:
         with open(report, "a") as f:
-            f.write(json.dumps({"workload": name, "storage": storage, "geometry": "fp64", "arith": "fast",
+            f.write(json.dumps({"workload": name, "storage": storage, "ratio": FORMS[storage][0],
+                                "images": FORMS[storage][1], "geometry": "fp64", "arith": "strict",
                                 "it": it, "sit": sit, "rel_rmse_vs_fp64": err, "rel_rmse_all": err_all,
                                 "voxels": int(np.isfinite(v64).sum()), "nan_mismatch": nan_mismatch}) + "\n")
     assert nan_mismatch <= 1e-5, nan_mismatch
-    assert err <= TOL[storage], (name, storage, err)
+    assert err <= TOL, (name, storage, err)

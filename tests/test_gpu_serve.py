@@ -95,7 +95,7 @@ def test_requests_in_flight_share_ticks(sctx):
 
 def test_served_equals_whole_run_entry_point(sctx):
     params, raw = _request(1)
-    srv = Server(sctx, storage=_lib.F32)
+    srv = Server(sctx, arith=_lib.STRICT, storage=_lib.F32)
     t = srv.submit(params, raw)
     assert srv.wait(t, 60.0).state == DONE
     got = srv.result(t)
@@ -106,7 +106,7 @@ def test_served_equals_whole_run_entry_point(sctx):
     P, H, W = raw.shape
     exp = np.full(got.size, np.nan, np.float32)
     cfg = json.loads(json.dumps(params))
-    cfg["recon"]["arith"] = "fast"
+    cfg["recon"]["arith"] = "strict"
     rc = L.xpr_reconstruct_host(json.dumps(cfg).encode(), raw.ctypes.data, P, W, H, exp.ctypes.data, exp.size,
                                 C.byref(C.c_double()))
     assert rc == 0

@@ -1,7 +1,8 @@
 """Slab sharding of one reconstruction over ranks (xpulse_recon_b200/shard.py) on the CPU:
-world_size 2 and 3 gloo process groups on 127.0.0.1, with the oracle as the arithmetic.
-The gathered volume must equal the single-process oracle reconstruction bit for bit
-(the exchanged sums are integers)."""
+world_size 2 and 3 gloo process groups on 127.0.0.1, with the oracle as the arithmetic,
+both with detector-row windows (point-to-point exchange of the shared rows, the default)
+and with the whole detector all-reduced.  The gathered volume must equal the
+single-process oracle reconstruction bit for bit (the exchanged sums are integers)."""
 import ctypes as C
 import os
 import socket
@@ -14,7 +15,8 @@ torch = pytest.importorskip("torch")
 from oracle import oracle as O  # noqa: E402
 from tests.cases import assert_same_bits  # noqa: E402
 from xpulse_recon_b200 import _lib  # noqa: E402
-from xpulse_recon_b200.shard import SlabReconstruction, slab_bounds  # noqa: E402
+from xpulse_recon_b200.shard import (SlabReconstruction, exchange_plan, exchange_rows, row_window,  # noqa: E402
+                                     slab_bounds)
 
 GEOM = dict(dwidth=40, dheight=32, projections=24, sit=4, rx=1.0, sx=-0.5, sy=0.8)
 
@@ -66,6 +68,9 @@ class OracleOps:
         t = torch.from_numpy(sums.view(np.int32))  # u32 addition modulo 2^32 == wrapping int32 addition
         dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
 
+    def exchange(self, sums, plan, r0, n_img, rows, width, group=None):
+        return exchange_rows(torch.from_numpy(sums.view(np.int32)), plan, r0, n_img, rows, width, group)
+
     def synchronize(self):
         pass
 
@@ -82,19 +87,22 @@ def _inputs():
     return raw, pd_all, g
 
 
-def _rank_main(rank, world, port, out_dir):
+def _rank_main(rank, world, port, out_dir, windowed):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         raw, pd_all, g = _inputs()
-        r = SlabReconstruction(OracleOps(), raw, pd_all, g, it=2, sit=GEOM["sit"], seed=77, rank=rank, world=world)
+        r = SlabReconstruction(OracleOps(), raw, pd_all, g, it=2, sit=GEOM["sit"], seed=77, rank=rank, world=world,
+                               windowed=windowed)
         r.run()
         vol = r.gather()
+        sent = [None] * world
+        dist.all_gather_object(sent, r.exchanged_bytes)
         if rank == 0:
             np.save(os.path.join(out_dir, "vol_%d.npy" % world), vol)
-            np.save(os.path.join(out_dir, "bytes_%d.npy" % world), np.array([r.exchanged_bytes]))
+            np.save(os.path.join(out_dir, "bytes_%d.npy" % world), np.array(sent))
     finally:
         dist.destroy_process_group()
 
@@ -114,10 +122,11 @@ def test_slab_bounds_partition():
             assert max(y1 - y0 for y0, y1 in b) - min(y1 - y0 for y0, y1 in b) <= 1
 
 
+@pytest.mark.parametrize("windowed", [True, False])
 @pytest.mark.parametrize("world", [2, 3])
-def test_sharded_equals_single_process(tmp_path, world):
+def test_sharded_equals_single_process(tmp_path, world, windowed):
     import torch.multiprocessing as mp
-    mp.spawn(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    mp.spawn(_rank_main, args=(world, _free_port(), str(tmp_path), windowed), nprocs=world, join=True)
     got = np.load(tmp_path / ("vol_%d.npy" % world))
     raw, pd_all, g = _inputs()
     imgs = raw.ravel().copy()
@@ -128,6 +137,39 @@ def test_sharded_equals_single_process(tmp_path, world):
     assert O.lib().orc_recon_naive(C.byref(gp), C.byref(rp), imgs, exp) == 0
     assert np.isfinite(got).mean() > 0.5
     assert_same_bits(got, exp)
-    # one exchange of the detector sums per sub-iteration with a forward
+    # one exchange per sub-iteration with a forward: the whole detector, or the shared rows
     npix = g["concurrent"] * GEOM["dwidth"] * GEOM["dheight"]
-    assert int(np.load(tmp_path / ("bytes_%d.npy" % world))[0]) == 4 * npix * (2 * GEOM["sit"] - 1)
+    sent = np.load(tmp_path / ("bytes_%d.npy" % world))
+    forwards = 2 * GEOM["sit"] - 1
+    if not windowed:
+        assert all(int(b) == 4 * npix * forwards for b in sent)
+    else:
+        windows = [row_window(pd_all, g, *slab_bounds(int(g["vheight"]), world, q), GEOM["dheight"])
+                   for q in range(world)]
+        for q in range(world):
+            shared = sum(b - a for _, a, b in exchange_plan(windows, q))
+            assert int(sent[q]) == 4 * g["concurrent"] * GEOM["dwidth"] * shared * forwards
+            assert shared < GEOM["dheight"]
+
+
+def test_row_windows_cover_every_voxel_pixel():
+    """Every in-bounds pixel a slab's voxels reach (oracle forward of the slab, all
+    projections, jittered origins) lies in the slab's row window."""
+    raw, pd_all, g = _inputs()
+    gp = O.geom_params(**GEOM)
+    W, Hv, Wd, Hd = int(g["vwidth"]), int(g["vheight"]), GEOM["dwidth"], GEOM["dheight"]
+    P = GEOM["projections"]
+    rng = np.random.default_rng(3)
+    for world in (2, 3, 5):
+        for q in range(world):
+            y0, y1 = slab_bounds(Hv, world, q)
+            r0, r1 = row_window(pd_all, g, y0, y1, Hd)
+            vol = np.ones(W * (y1 - y0) * W, np.float32)
+            for _ in range(3):
+                origin = [float(np.float32(g["orig"][i]) + np.float32(rng.uniform(0, g["vx"]))) for i in range(3)]
+                L, keep = O.make_launch((0, y0, 0), (W, y1, W), origin, [g["vx"]] * 3, Wd, Hd, 0, P, 1, arith=O.FAST)
+                sums = np.zeros(P * Wd * Hd, np.uint32)
+                O.forward(vol, sums, np.ascontiguousarray(pd_all), L)
+                hit = sums.reshape(P, Hd, Wd).any(axis=(0, 2))
+                rows = np.nonzero(hit)[0]
+                assert rows.min() >= r0 and rows.max() < r1, (world, q, rows.min(), rows.max(), r0, r1)

@@ -28,7 +28,17 @@ def _signatures(L):
     L.xpr_subiteration_static_capacity.argtypes = []
 
 
-def test_static_scratch_subiteration_matches_allocating_entry():
+TORCH_DT = {_lib.F32: torch.float32, _lib.BF16: torch.bfloat16, _lib.F16: torch.float16}
+
+
+@pytest.mark.parametrize("image_dtype,arith,lists", [
+    (_lib.F32, _lib.FAST, False),
+    (_lib.F32, _lib.STRICT, False),
+    (_lib.BF16, _lib.FAST, False),
+    (_lib.F16, _lib.STRICT, False),
+    (_lib.F32, _lib.STRICT, True),   # ForwardH / BackwardH index lists
+])
+def test_static_scratch_subiteration_matches_allocating_entry(image_dtype, arith, lists):
     L = _lib.lib()
     _signatures(L)
     ctx = Context(0)
@@ -42,8 +52,12 @@ def test_static_scratch_subiteration_matches_allocating_entry():
         raw = rng.uniform(0.05, 0.95, (kw["projections"], Hd, Wd)).astype(np.float32)
         meas = (-np.log(raw)).astype(np.float32)
         imgs = [torch.from_numpy(np.ascontiguousarray(meas[[s + k * S for k in range(Pc)]]).ravel()).cuda()
-                for s in range(S)]
+                .to(TORCH_DT[image_dtype]) for s in range(S)]
         pds = [torch.from_numpy(np.ascontiguousarray(pd_all[[s + k * S for k in range(Pc)]])).cuda() for s in range(S)]
+        keep = []
+        if lists:  # every entry but one, in reverse order: entry i -> ProjData and image slot Pc - 1 - i
+            order = np.arange(Pc - 1, 0, -1, dtype=np.uint16)
+            keep = [torch.from_numpy(order.copy()).cuda(), torch.from_numpy(order.copy()).cuda()]
         vol_alloc = torch.ones(W * Hv * W, dtype=torch.float32, device="cuda")
         vol_static = torch.ones_like(vol_alloc)
         sums = torch.full((n,), 1 << 22, dtype=torch.int32, device="cuda")  # the caller's scratch
@@ -55,14 +69,18 @@ def test_static_scratch_subiteration_matches_allocating_entry():
             Ld.origin[:] = [g["orig"][i] + 0.3 * g["vx"] * (call + 1) for i in range(3)]
             Ld.voxel[:] = [g["vx"]] * 3
             Ld.det_w, Ld.rows, Ld.row_offset, Ld.n_angles, Ld.modules = Wd, Hd, 0, Pc, 1
-            Ld.arith = _lib.FAST
+            Ld.arith = arith
+            if lists:
+                Ld.list_mvp, Ld.list_img, Ld.n_list = keep[0].data_ptr(), keep[1].data_ptr(), keep[0].numel()
             first = 1 if call == 0 else 0
+            if first:
+                sums.fill_(1 << 22)
             _lib.check(L.xpr_subiteration(ctx.handle, vol_alloc.data_ptr(), sums.data_ptr(), imgs[sit].data_ptr(),
-                                          _lib.F32, sums.data_ptr(), _lib.F32, pds[sit].data_ptr(), Pc, C.byref(Ld),
-                                          1.0, first, None, stream), "xpr_subiteration")
-            _lib.check(L.xpr_subiteration_static(ctx.handle, vol_static.data_ptr(), imgs[sit].data_ptr(), _lib.F32,
-                                                 pds[sit].data_ptr(), Pc, C.byref(Ld), 1.0, first, stream),
-                       "xpr_subiteration_static")
+                                          image_dtype, sums.data_ptr(), _lib.F32, pds[sit].data_ptr(), Pc,
+                                          C.byref(Ld), 1.0, first, None, stream), "xpr_subiteration")
+            _lib.check(L.xpr_subiteration_static(ctx.handle, vol_static.data_ptr(), imgs[sit].data_ptr(),
+                                                 image_dtype, pds[sit].data_ptr(), Pc, C.byref(Ld), 1.0, first,
+                                                 stream), "xpr_subiteration_static")
             torch.cuda.synchronize()
             # the tolerance of this suite's FP32 path: identical bits (NaN positions identical)
             assert_same_bits(vol_static.cpu().numpy(), vol_alloc.cpu().numpy())
@@ -74,9 +92,9 @@ def test_static_scratch_subiteration_matches_allocating_entry():
         Lbig.vmax[:] = [W, Hv, W]
         Lbig.voxel[:] = [g["vx"]] * 3
         Lbig.det_w, Lbig.rows, Lbig.n_angles, Lbig.modules = 4096, 4096, 1, 1
-        rc = L.xpr_subiteration_static(ctx.handle, vol_static.data_ptr(), imgs[0].data_ptr(), _lib.F32,
+        rc = L.xpr_subiteration_static(ctx.handle, vol_static.data_ptr(), imgs[0].data_ptr(), image_dtype,
                                        pds[0].data_ptr(), Pc, C.byref(Lbig), 1.0, 1, stream)
-        assert rc == 4  # XPR_ERR_CAP
+        assert rc == _lib.ERR_CAP
         assert b"static scratch" in L.xpr_last_error()
     finally:
         ctx.close()

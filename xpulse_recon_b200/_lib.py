@@ -12,6 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libxpr.so")
 
 XPR_OK = 0
+# status codes (enum xpr_status)
+ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_CAP, ERR_IO, ERR_PARAM, ERR_UNSUPPORTED = 1, 2, 3, 4, 5, 6, 7
 STRICT, FAST = 0, 1
 F32, BF16, F16 = 0, 1, 2
 ERROR_STD, ERROR_FIRST_1C, ERROR_1C = 0, 1, 2
@@ -65,7 +67,8 @@ class BatchProblem(C.Structure):
 class BatchOpts(C.Structure):
     _fields_ = [("arith", C.c_int32), ("storage", C.c_int32), ("init_volume", C.c_int32),
                 ("use_graph", C.c_int32), ("autotune", C.c_int32), ("fwd_splits", C.c_int32),
-                ("bwd_column", C.c_int32), ("ctas_per_sm", C.c_int32)]
+                ("bwd_column", C.c_int32), ("ctas_per_sm", C.c_int32), ("image_storage_set", C.c_int32),
+                ("image_storage", C.c_int32)]
 
 
 _lib = None

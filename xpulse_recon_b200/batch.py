@@ -28,7 +28,7 @@ def torch_dtype(storage: int):
 class Problem:
     """One naive reconstruction resident on the device."""
     vol: object                    # torch float32 [vheight * vwidth * vwidth]
-    images: object                 # torch [sit * per_subset * det_h * det_w], storage dtype, subset-major
+    images: object                 # torch [sit * per_subset * det_h * det_w], image storage dtype, subset-major
     projdata: object               # torch float32 [sit * per_subset * modules, 20], subset-major
     det_w: int
     det_h: int
@@ -50,7 +50,8 @@ class Problem:
     def from_raw(ctx: Context, raw: np.ndarray, geom: dict, it: int, sit: int, seed: int = 5489,
                  weight: float = 1.0, weight_factor: float = 0.9, storage: int = _lib.F32, mlog: bool = True,
                  fp64_geometry: bool = False, residual: bool = False) -> "Problem":
-        """raw: (projections, det_h, det_w) float32 intensities in acquisition order."""
+        """raw: (projections, det_h, det_w) float32 intensities in acquisition order;
+        storage: the dtype the preprocessed images are kept in."""
         import torch
         P, H, W = raw.shape
         M = int(geom.get("module_number", 1))
@@ -82,9 +83,10 @@ class Problem:
         p.residual = None if self.residual is None else self.residual.data_ptr()
         return p
 
-    def run_alone(self, ctx: Context, arith: int = _lib.FAST, storage: int = _lib.F32) -> None:
+    def run_alone(self, ctx: Context, arith: int = _lib.STRICT, storage: int = _lib.F32) -> None:
         """The same reconstruction without the batch: one xpr_subiteration per
-        sub-iteration (reconstruction_n.hpp:65-76), from a fresh volume of 1.0."""
+        sub-iteration (reconstruction_n.hpp:65-76), from a fresh volume of 1.0;
+        storage is the ratio's dtype (the images keep theirs)."""
         import torch
         L = lib()
         self.vol.fill_(1.0)
@@ -97,6 +99,7 @@ class Problem:
         check(L.xpr_jitter(self.seed, jit.size, self.voxel, jit.ctypes.data), "xpr_jitter")
         w = np.float32(self.weight)
         isz = self.images.element_size()
+        idt = {torch.float32: _lib.F32, torch.bfloat16: _lib.BF16, torch.float16: _lib.F16}[self.images.dtype]
         for k in range(steps):
             s = k % self.sit
             d = _lib.Launch()
@@ -107,7 +110,7 @@ class Problem:
                 self.modules, arith
             res = None if self.residual is None else self.residual.data_ptr() + 8 * k
             check(L.xpr_subiteration(ctx.handle, self.vol.data_ptr(), sums.data_ptr(),
-                                     self.images.data_ptr() + s * npix * isz, storage, ratio.data_ptr(), storage,
+                                     self.images.data_ptr() + s * npix * isz, idt, ratio.data_ptr(), storage,
                                      self.projdata.data_ptr() + s * E * 80, E, C.byref(d), float(w), int(k == 0),
                                      res, _stream()), "xpr_subiteration")
             if s == self.sit - 1:
@@ -117,13 +120,15 @@ class Problem:
 class Batch:
     """xpr_batch handle over a list of Problems (kept alive with it)."""
 
-    def __init__(self, ctx: Context, problems: list, arith: int = _lib.FAST, storage: int = _lib.F32,
+    def __init__(self, ctx: Context, problems: list, arith: int = _lib.STRICT, storage: int = _lib.F32,
                  init_volume: bool = True, use_graph: bool = True, autotune: bool = True, fwd_splits: int = 0,
-                 bwd_column: int = 0, ctas_per_sm: int = 0):
+                 bwd_column: int = 0, ctas_per_sm: int = 0, image_storage: int = None):
+        """storage: the ratio's dtype, and the images' unless image_storage is given."""
         self.ctx, self.problems = ctx, list(problems)
         arr = (_lib.BatchProblem * len(self.problems))(*[p.c_struct() for p in self.problems])
         o = _lib.BatchOpts(arith, storage, int(init_volume), int(use_graph), int(autotune), fwd_splits, bwd_column,
-                           ctas_per_sm)
+                           ctas_per_sm, int(image_storage is not None),
+                           storage if image_storage is None else image_storage)
         h = C.c_void_p()
         check(lib().xpr_batch_create(ctx.handle, arr, len(self.problems), C.byref(o), _stream(), C.byref(h)),
               "xpr_batch_create")

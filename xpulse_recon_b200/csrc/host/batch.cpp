@@ -35,7 +35,7 @@ struct StepPlan {
 };
 
 // tuned schedules, per batch shape
-using ShapeKey = std::tuple<int, int, std::vector<uint64_t>>;
+using ShapeKey = std::tuple<int, int, int, std::vector<uint64_t>>;
 std::mutex g_tune_mu;
 std::map<ShapeKey, std::tuple<int, int, double>> g_tuned;
 
@@ -94,7 +94,7 @@ int build_lists(xpr_batch *b, int splits, int column, cudaStream_t s)
         StepPlan &P = b->plan[k];
         it.clear();
         for (const auto &pp : b->probs)
-            if (k < pp.steps() && !xpr::add_step_items(pp, k, splits, column, b->opts.storage, &it))
+            if (k < pp.steps() && !xpr::add_step_items(pp, k, splits, column, b->opts.image_storage, &it))
                 return fail(XPR_ERR_UNSUPPORTED, "batch step exceeds 2^31 work units");
         P.n_fwd = (int)it.fwd.size();
         P.n_err = (int)it.err.size();
@@ -159,7 +159,7 @@ cudaError_t enqueue_step(xpr_batch *b, uint32_t k, cudaStream_t s)
     cudaError_t e = enqueue_forward(b, k, s);
     if (e == cudaSuccess && P.n_err)
         e = xpr::launch_error_batched((const xpr::BatchErrItem *)((char *)b->lists + P.err_off), P.n_err,
-                                      b->opts.storage, b->opts.storage, P.max_n, *b->di, s);
+                                      b->opts.image_storage, b->opts.storage, P.max_n, *b->di, s);
     if (e == cudaSuccess) e = enqueue_backward(b, k, s);
     return e;
 }
@@ -212,7 +212,7 @@ int autotune(xpr_batch *b, cudaStream_t s)
         max_e = std::max(max_e, xpr::entries_of(p));
         shape.insert(shape.end(), {p.vwidth, p.vheight, p.det_w, p.det_h, p.per_subset, p.modules});
     }
-    const ShapeKey key{b->opts.arith, b->opts.storage, shape};
+    const ShapeKey key{b->opts.arith, b->opts.storage, b->opts.image_storage, shape};
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tuned.find(key);
@@ -289,6 +289,9 @@ int xpr_batch_create(xpr_ctx *ctx, const xpr_batch_problem *problems, uint32_t n
     if (o.arith != XPR_ARITH_STRICT && o.arith != XPR_ARITH_FAST) return fail(XPR_ERR_INVALID, "unknown arith");
     if (o.storage != XPR_F32 && o.storage != XPR_BF16 && o.storage != XPR_F16)
         return fail(XPR_ERR_INVALID, "unknown storage dtype");
+    if (!o.image_storage_set) o.image_storage = o.storage;
+    if (o.image_storage != XPR_F32 && o.image_storage != XPR_BF16 && o.image_storage != XPR_F16)
+        return fail(XPR_ERR_INVALID, "unknown image storage dtype");
     if (o.bwd_column != 0 && o.bwd_column != 8 && o.bwd_column != 16)
         return fail(XPR_ERR_INVALID, "bwd_column must be 0, 8 or 16");
     cudaError_t e = xpr::prepare_device_kernels();
@@ -385,6 +388,7 @@ int xpr_batch_step(xpr_batch *b, uint32_t step, void *stream)
     if (!b) return fail(XPR_ERR_INVALID, "xpr_batch_step: NULL batch");
     if (step >= b->steps) return fail(XPR_ERR_INVALID, "xpr_batch_step: step out of range");
     if (!xpr::context_device(b->ctx)) return XPR_ERR_INVALID;
+    xpr::Range nvtx("xpr.batch_step");
     const cudaError_t e = enqueue_step(b, step, reinterpret_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? XPR_OK : cuda_fail(e, "xpr_batch_step");
 }
@@ -393,6 +397,7 @@ int xpr_batch_run(xpr_batch *b, void *stream)
 {
     if (!b) return fail(XPR_ERR_INVALID, "xpr_batch_run: NULL batch");
     if (!xpr::context_device(b->ctx)) return XPR_ERR_INVALID;
+    xpr::Range nvtx("xpr.batch_run");
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     if (!b->opts.use_graph) {
         const cudaError_t e = enqueue_run(b, s);

@@ -39,7 +39,7 @@ const char *plan_problem(const xpr_batch_problem &p, int arith, PlannedProblem *
     return nullptr;
 }
 
-bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int column, int storage, StepItems *out)
+bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int column, int image_dtype, StepItems *out)
 {
     const xpr_batch_problem &p = pp.p;
     const uint32_t s_idx = k % p.sit;
@@ -65,7 +65,7 @@ bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int column
         out->fwd.push_back(f);
     }
     BatchErrItem e{};
-    e.images = (const char *)p.images + (size_t)s_idx * npix * dtype_size(storage);
+    e.images = (const char *)p.images + (size_t)s_idx * npix * dtype_size(image_dtype);
     e.sum = pp.sums;
     e.ratio = pp.ratio;
     e.residual = p.residual ? p.residual + k : nullptr;

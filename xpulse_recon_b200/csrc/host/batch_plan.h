@@ -54,6 +54,6 @@ struct StepItems {
 
 // Appends sub-iteration k of `pp` (k < pp.steps()); false when the step would exceed 2^31
 // work units.  splits: projection runs per forward brick; column: backward column length.
-bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int column, int storage, StepItems *out);
+bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int column, int image_dtype, StepItems *out);
 
 }  // namespace xpr

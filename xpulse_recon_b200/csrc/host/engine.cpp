@@ -184,8 +184,8 @@ struct Engine::Impl {
     std::vector<xpr_projdata> pd_all;
     std::vector<float> mod_offset, mod_rpy;
     std::mt19937 rng;
-    int arith = XPR_ARITH_FAST, dtype = XPR_F32;
-    uint64_t esize = 4;
+    int arith = XPR_ARITH_FAST, idt = XPR_F32, rdt = XPR_F32;  // image / ratio storage
+    uint64_t iesize = 4, rsize = 4;                            // their element sizes
     int64_t P = 0, S = 0, Pc = 0, M = 1, slots = 0, W = 0, Hv = 0, Wd = 0, Hd = 0;
     uint64_t WH = 0, N = 0;
     float nmin = FLT_MAX, nmax = FLT_MIN;
@@ -224,7 +224,7 @@ struct Engine::Impl {
     void preprocess(const Params &p, const std::function<void(int64_t, const void *)> &sink)
     {
         DevBuf raw[2] = {DevBuf(ctx, WH * 4), DevBuf(ctx, WH * 4)};
-        DevBuf out[2] = {DevBuf(ctx, WH * esize), DevBuf(ctx, WH * esize)};
+        DevBuf out[2] = {DevBuf(ctx, WH * iesize), DevBuf(ctx, WH * iesize)};
         DevBuf mm(ctx, 8);
         PinBuf stage0(ctx, WH * 4), stage1(ctx, WH * 4);
         PinBuf *stage[2] = {&stage0, &stage1};
@@ -254,7 +254,7 @@ struct Engine::Impl {
         }
         for (int64_t i = 0; i < P; ++i) {
             const int b = next(i);
-            check(xpr_preprocess_apply(ctx, raw[b].as<float>(), out[b].p, dtype, WH, p.normalize ? 1 : 0,
+            check(xpr_preprocess_apply(ctx, raw[b].as<float>(), out[b].p, idt, WH, p.normalize ? 1 : 0,
                                        mm.as<float>(), p.mlog ? 1 : 0, comp->v()), "preprocess");
             sink(i, out[b].p);
             used[b].record(*comp);
@@ -353,8 +353,11 @@ Engine::Engine(const Params &p, std::unique_ptr<ImageSource> images, bool write_
     if (p.seed_set) d.rng.seed(p.seed);
     else d.rng.seed(std::random_device()());
     d.arith = p.arith == "strict" ? XPR_ARITH_STRICT : XPR_ARITH_FAST;
-    d.dtype = p.storage == "bf16" ? XPR_BF16 : (p.storage == "fp16" ? XPR_F16 : XPR_F32);
-    d.esize = d.dtype == XPR_F32 ? 4 : 2;
+    d.rdt = p.storage == "bf16" ? XPR_BF16 : (p.storage == "fp16" ? XPR_F16 : XPR_F32);
+    d.idt = p.image_storage.empty() ? d.rdt
+               : (p.image_storage == "bf16" ? XPR_BF16 : (p.image_storage == "fp16" ? XPR_F16 : XPR_F32));
+    d.iesize = d.idt == XPR_F32 ? 4 : 2;
+    d.rsize = d.rdt == XPR_F32 ? 4 : 2;
     // dataset.hpp:214-235
     d.P = d.src->count();
     d.Wd = d.src->width();
@@ -401,19 +404,19 @@ void Engine::reconstruct()
 
     if (p.method == Method::naive) {
         const uint64_t nvol = p.compat_pad ? xpr_ndrange(N) : N;
-        const bool sep = d.dtype != XPR_F32;
-        const uint64_t need = nvol * 4 + (uint64_t)(S * Pc) * WH * d.esize + Pc * WH * 4 + (sep ? Pc * WH * d.esize : 0) +
+        const bool sep = d.rdt != XPR_F32;
+        const uint64_t need = nvol * 4 + (uint64_t)(S * Pc) * WH * d.iesize + Pc * WH * 4 + (sep ? Pc * WH * d.rsize : 0) +
                               (uint64_t)(S * Pc * M) * PDB;
         std::cout << "Checking GPU memory requierments : " << need / (1024 * 1024) << "Mo" << std::endl;
         if (need > d.available()) throw std::runtime_error("Not enough GPU memory");
-        DevBuf img(d.ctx, (uint64_t)(S * Pc) * WH * d.esize), vol(d.ctx, nvol * 4), sum(d.ctx, Pc * WH * 4);
-        DevBuf ratio = sep ? DevBuf(d.ctx, Pc * WH * d.esize) : DevBuf();
+        DevBuf img(d.ctx, (uint64_t)(S * Pc) * WH * d.iesize), vol(d.ctx, nvol * 4), sum(d.ctx, Pc * WH * 4);
+        DevBuf ratio = sep ? DevBuf(d.ctx, Pc * WH * d.rsize) : DevBuf();
         DevBuf pd(d.ctx, (uint64_t)(S * Pc * M) * PDB);
         std::cout << "Pre-processing images..." << std::flush;
         d.preprocess(p, [&](int64_t i, const void *dimg) {
             if (i / S >= Pc) return;  // the kernels use the first Pc angles of a sub-iteration
             const uint64_t slot = (uint64_t)((i % S) * Pc + i / S);
-            check_cuda(cudaMemcpyAsync(img.at(slot * WH * d.esize), dimg, WH * d.esize, cudaMemcpyDeviceToDevice,
+            check_cuda(cudaMemcpyAsync(img.at(slot * WH * d.iesize), dimg, WH * d.iesize, cudaMemcpyDeviceToDevice,
                                        d.comp->s), "copy");
         });
         std::cout << "Ok." << std::endl;
@@ -431,8 +434,8 @@ void Engine::reconstruct()
                                         p.compat_pad ? 1 : 0);
                 const bool first = (mit == 0 && sit == 0);
                 check(xpr_subiteration(d.ctx, vol.as<float>(), sum.as<uint32_t>(),
-                                       img.at((uint64_t)sit * Pc * WH * d.esize), d.dtype, sep ? ratio.p : sum.p,
-                                       d.dtype, (const xpr_projdata *)pd.at((uint64_t)sit * Pc * M * PDB),
+                                       img.at((uint64_t)sit * Pc * WH * d.iesize), d.idt, sep ? ratio.p : sum.p,
+                                       d.rdt, (const xpr_projdata *)pd.at((uint64_t)sit * Pc * M * PDB),
                                        (uint32_t)(Pc * M), &L, weight, first ? 1 : 0, nullptr, d.comp->v()),
                       "sub-iteration");
                 stats_.subiterations++;
@@ -457,12 +460,12 @@ void Engine::reconstruct()
         const bool lplh = p.method == Method::method_1c;
         const bool sync_mode = p.method == Method::method_1a;
         const int64_t slots = lplh ? d.slots : Pc;
-        const bool sep = d.dtype != XPR_F32;
+        const bool sep = d.rdt != XPR_F32;
         PinBuf hvol(d.ctx, N * 4);
-        PinBuf himg(d.ctx, (uint64_t)(S * slots) * WH * d.esize);
+        PinBuf himg(d.ctx, (uint64_t)(S * slots) * WH * d.iesize);
         // device: one sub-iteration's images and sums, ProjData, lists, slab buffers
-        DevBuf img(d.ctx, (uint64_t)slots * WH * d.esize), sum(d.ctx, (uint64_t)slots * WH * 4);
-        DevBuf ratio = sep ? DevBuf(d.ctx, (uint64_t)slots * WH * d.esize) : DevBuf();
+        DevBuf img(d.ctx, (uint64_t)slots * WH * d.iesize), sum(d.ctx, (uint64_t)slots * WH * 4);
+        DevBuf ratio = sep ? DevBuf(d.ctx, (uint64_t)slots * WH * d.rsize) : DevBuf();
         DevBuf pd, lm, li;
         std::vector<uint16_t> hl_m, hl_i;
         if (lplh) {
@@ -493,7 +496,7 @@ void Engine::reconstruct()
         std::cout << "Pre-processing images..." << std::flush;
         d.preprocess(p, [&](int64_t i, const void *dimg) {
             if (i / S >= slots) return;
-            check_cuda(cudaMemcpyAsync(himg.at((uint64_t)((i % S) * slots + i / S) * WH * d.esize), dimg, WH * d.esize,
+            check_cuda(cudaMemcpyAsync(himg.at((uint64_t)((i % S) * slots + i / S) * WH * d.iesize), dimg, WH * d.iesize,
                                        cudaMemcpyDeviceToHost, d.comp->s), "copy");
         });
         std::cout << "Ok." << std::endl;
@@ -521,8 +524,8 @@ void Engine::reconstruct()
                 for (int64_t sit = 0; sit < S; ++sit) {
                     d.jittered_origin(go_, origin);
                     const bool first = (mit == 0 && sit == 0);
-                    check(xpr_upload(d.ctx, img.p, himg.at((uint64_t)sit * slots * WH * d.esize),
-                                     (uint64_t)Pc * WH * d.esize, d.comp->v()), "upload");
+                    check(xpr_upload(d.ctx, img.p, himg.at((uint64_t)sit * slots * WH * d.iesize),
+                                     (uint64_t)Pc * WH * d.iesize, d.comp->v()), "upload");
                     const void *pdp = pd.at((uint64_t)sit * Pc * M * PDB);
                     if (!first) {
                         for (int64_t j = 0; j < nslab; ++j) {
@@ -536,7 +539,7 @@ void Engine::reconstruct()
                             stats_.pairs += (uint64_t)ny * W * W * Pc;
                         }
                     }
-                    check(xpr_error(d.ctx, img.p, d.dtype, sum.as<uint32_t>(), sep ? ratio.p : sum.p, d.dtype,
+                    check(xpr_error(d.ctx, img.p, d.idt, sum.as<uint32_t>(), sep ? ratio.p : sum.p, d.rdt,
                                     (uint64_t)Pc * WH, weight, XPR_ERROR_STD, 0, nullptr, d.comp->v()), "error");
                     for (int64_t j = 0; j < nslab; ++j) {
                         const int64_t y0 = j * slab, ny = std::min<int64_t>(Hv, (j + 1) * slab) - y0;
@@ -544,7 +547,7 @@ void Engine::reconstruct()
                                          d.comp->v()), "upload");
                         xpr_launch L = d.launch((int32_t)y0, (int32_t)(y0 + ny), origin, go_.vx, (uint32_t)d.Hd, 0,
                                                 (uint32_t)Pc, 0);
-                        check(xpr_backward(d.ctx, sb.as<float>(), sep ? ratio.p : sum.p, d.dtype,
+                        check(xpr_backward(d.ctx, sb.as<float>(), sep ? ratio.p : sum.p, d.rdt,
                                            (const xpr_projdata *)pdp, (uint32_t)(Pc * M), &L, d.comp->v()),
                               "backward");
                         stats_.pairs += (uint64_t)ny * W * W * Pc;
@@ -632,8 +635,8 @@ void Engine::reconstruct()
                     d.jittered_origin(go_, origin);
                     const bool first = (mit == 0 && sit == 0);
                     const int64_t nimg = lplh ? d.angles_in(sit) : Pc;
-                    check(xpr_upload(d.ctx, img.p, himg.at((uint64_t)sit * slots * WH * d.esize),
-                                     (uint64_t)nimg * WH * d.esize, d.comp->v()), "upload");
+                    check(xpr_upload(d.ctx, img.p, himg.at((uint64_t)sit * slots * WH * d.iesize),
+                                     (uint64_t)nimg * WH * d.iesize, d.comp->v()), "upload");
                     const void *pdp = lplh ? pd.p : pd.at((uint64_t)sit * Pc * M * PDB);
                     const uint32_t npd = lplh ? (uint32_t)d.pd_all.size() : (uint32_t)(Pc * M);
                     auto slab_launch = [&](int64_t j) {
@@ -662,14 +665,14 @@ void Engine::reconstruct()
                     }
                     // ---- error
                     const int mode = lplh ? (first ? XPR_ERROR_FIRST_1C : XPR_ERROR_1C) : XPR_ERROR_STD;
-                    check(xpr_error(d.ctx, img.p, d.dtype, sum.as<uint32_t>(), sep ? ratio.p : sum.p, d.dtype,
+                    check(xpr_error(d.ctx, img.p, d.idt, sum.as<uint32_t>(), sep ? ratio.p : sum.p, d.rdt,
                                     (uint64_t)nimg * WH, weight, mode, 0, nullptr, d.comp->v()), "error");
                     // ---- backward over the slabs, descending
                     for (int64_t j = nslab - 1; j >= 0; --j) {
                         SlabBuf &b = acquire(j);
                         xpr_launch L = slab_launch(j);
                         L.nan_skip = lplh ? 1 : 0;
-                        check(xpr_backward(d.ctx, b.mem.as<float>(), sep ? ratio.p : sum.p, d.dtype,
+                        check(xpr_backward(d.ctx, b.mem.as<float>(), sep ? ratio.p : sum.p, d.rdt,
                                            (const xpr_projdata *)pdp, npd, &L, d.comp->v()), "backward");
                         b.used.record(*d.comp);
                         b.used_rec = true;
@@ -714,12 +717,12 @@ void Engine::reconstruct()
             for (int64_t l = 0; l < Hv; ++l)
                 if (!covered[(size_t)l]) std::fill(vout + (uint64_t)l * W * W, vout + (uint64_t)(l + 1) * W * W, NAN);
         }
-        const bool sep = d.dtype != XPR_F32;
-        PinBuf himg(d.ctx, (uint64_t)(S * Pc) * WH * d.esize);
+        const bool sep = d.rdt != XPR_F32;
+        PinBuf himg(d.ctx, (uint64_t)(S * Pc) * WH * d.iesize);
         std::cout << "Pre-processing images..." << std::flush;
         d.preprocess(p, [&](int64_t i, const void *dimg) {
             if (i / S >= Pc) return;
-            check_cuda(cudaMemcpyAsync(himg.at((uint64_t)((i % S) * Pc + i / S) * WH * d.esize), dimg, WH * d.esize,
+            check_cuda(cudaMemcpyAsync(himg.at((uint64_t)((i % S) * Pc + i / S) * WH * d.iesize), dimg, WH * d.iesize,
                                        cudaMemcpyDeviceToHost, d.comp->s), "copy");
         });
         std::cout << "Ok." << std::endl;
@@ -734,8 +737,8 @@ void Engine::reconstruct()
             const int64_t y0 = c.vOffset - c.vPadTop, ny = c.vPadTop + c.vSize + c.vPadBot;
             const uint64_t rows = (uint64_t)c.iSize, cw = (uint64_t)d.Wd * rows;
             DevBuf slab(d.ctx, (uint64_t)ny * W * W * 4);
-            DevBuf img(d.ctx, (uint64_t)Pc * cw * d.esize), sum(d.ctx, (uint64_t)Pc * cw * 4);
-            DevBuf ratio = sep ? DevBuf(d.ctx, (uint64_t)Pc * cw * d.esize) : DevBuf();
+            DevBuf img(d.ctx, (uint64_t)Pc * cw * d.iesize), sum(d.ctx, (uint64_t)Pc * cw * 4);
+            DevBuf ratio = sep ? DevBuf(d.ctx, (uint64_t)Pc * cw * d.rsize) : DevBuf();
             check(xpr_fill_u32(d.ctx, slab.p, 0x3f800000u, (uint64_t)ny * W * W, d.comp->v()), "fill");
             check(xpr_fill_u32(d.ctx, sum.p, 1u << 22, (uint64_t)Pc * cw, d.comp->v()), "fill");
             float weight = p.weight;
@@ -743,15 +746,15 @@ void Engine::reconstruct()
                 for (int64_t sit = 0; sit < S; ++sit) {
                     // the chunk's detector-row window of this sub-iteration's images
                     for (int64_t k = 0; k < Pc; ++k)
-                        check(xpr_upload(d.ctx, img.at((uint64_t)k * cw * d.esize),
-                                         himg.at(((uint64_t)(sit * Pc + k) * WH + (uint64_t)c.iOffset * d.Wd) * d.esize),
-                                         cw * d.esize, d.comp->v()), "upload");
+                        check(xpr_upload(d.ctx, img.at((uint64_t)k * cw * d.iesize),
+                                         himg.at(((uint64_t)(sit * Pc + k) * WH + (uint64_t)c.iOffset * d.Wd) * d.iesize),
+                                         cw * d.iesize, d.comp->v()), "upload");
                     d.jittered_origin(go_, origin);
                     xpr_launch L = d.launch((int32_t)y0, (int32_t)(y0 + ny), origin, go_.vx, (uint32_t)rows,
                                             (int32_t)c.iOffset, (uint32_t)Pc, 0);
                     const bool first = (mit == 0 && sit == 0);
-                    check(xpr_subiteration(d.ctx, slab.as<float>(), sum.as<uint32_t>(), img.p, d.dtype,
-                                           sep ? ratio.p : sum.p, d.dtype,
+                    check(xpr_subiteration(d.ctx, slab.as<float>(), sum.as<uint32_t>(), img.p, d.idt,
+                                           sep ? ratio.p : sum.p, d.rdt,
                                            (const xpr_projdata *)pd.at((uint64_t)sit * Pc * M * PDB), (uint32_t)(Pc * M),
                                            &L, weight, first ? 1 : 0, nullptr, d.comp->v()), "sub-iteration");
                     stats_.subiterations++;

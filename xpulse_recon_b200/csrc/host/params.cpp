@@ -104,6 +104,11 @@ Params params_from_json(const json::Value &root)
         if (p.storage != "fp32" && p.storage != "bf16" && p.storage != "fp16")
             throw std::runtime_error("recon.storage must be fp32|bf16|fp16");
     });
+    opt(r, "image_storage", [&](const json::Value &v) {
+        p.image_storage = str(v, "image_storage");
+        if (p.image_storage != "fp32" && p.image_storage != "bf16" && p.image_storage != "fp16")
+            throw std::runtime_error("recon.image_storage must be fp32|bf16|fp16");
+    });
     opt(r, "geometry", [&](const json::Value &v) {
         p.geometry = str(v, "geometry");
         if (p.geometry != "fp32" && p.geometry != "fp64") throw std::runtime_error("recon.geometry must be fp32|fp64");
@@ -205,7 +210,9 @@ std::string params_to_json(const Params &p)
       << ",\"weight_factor\":" << fnum(p.weight_factor) << ",\"normalize\":" << b(p.normalize)
       << ",\"simulation\":" << b(p.simulation);
     if (p.seed_set) o << ",\"seed\":" << p.seed;
-    o << ",\"arith\":\"" << p.arith << "\",\"storage\":\"" << p.storage << "\",\"geometry\":\"" << p.geometry
+    o << ",\"arith\":\"" << p.arith << "\",\"storage\":\"" << p.storage << "\"";
+    if (!p.image_storage.empty()) o << ",\"image_storage\":\"" << p.image_storage << "\"";
+    o << ",\"geometry\":\"" << p.geometry
       << "\",\"compat_pad\":" << b(p.compat_pad) << ",\"mem_cap\":" << p.mem_cap << ",\"device\":" << p.device
       << ",\"slab\":" << p.slab << ",\"slab_cache\":" << p.slab_cache << "}";
     o << ",\"geometry\":{\"so\":" << fnum(p.so) << ",\"sd\":" << fnum(p.sd) << ",\"angle\":" << fnum(p.angle)

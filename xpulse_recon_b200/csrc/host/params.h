@@ -5,8 +5,11 @@
 // (a path, or inline JSON when the argument starts with '{'; rx is converted from
 // pixels to mm after loading).  Extensions of this backend (all optional):
 //   recon.seed           origin-jitter seed (absent: std::random_device, as the reference)
-//   recon.arith          "fast" | "strict"  projector arithmetic contract
-//   recon.storage        "fp32" | "bf16" | "fp16"  detector image / ratio storage
+//   recon.arith          "strict" | "fast"  projector arithmetic contract (strict: the
+//                        reference kernels' IEEE single-precision results, bit for bit)
+//   recon.storage        "fp32" | "bf16" | "fp16"  ratio storage, and the measured images'
+//                        unless recon.image_storage is set
+//   recon.image_storage  "fp32" | "bf16" | "fp16"  storage of the preprocessed measured images
 //   recon.geometry       "fp32" | "fp64"  precision of the matrix construction (fp32: the
 //                        reference's single-precision glm construction, the default)
 //   recon.compat_pad     reproduce the reference's NDRange padding work-items (naive)
@@ -70,8 +73,9 @@ struct Params {
     // extensions
     bool seed_set = false;
     uint32_t seed = 0;
-    std::string arith = "fast";
+    std::string arith = "strict";
     std::string storage = "fp32";
+    std::string image_storage;  // empty: as storage
     std::string geometry = "fp32";
     bool compat_pad = false;
     uint64_t mem_cap = 0;

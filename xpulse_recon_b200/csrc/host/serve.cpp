@@ -74,7 +74,8 @@ struct xpr_server {
     xpr_ctx *ctx = nullptr;
     const xpr::DeviceInfo *di = nullptr;
     xpr_serve_opts opts{};
-    size_t esize = 4;
+    size_t esize = 4;   // ratio element bytes
+    size_t iesize = 4;  // image element bytes
     std::chrono::steady_clock::time_point t0;
     // state
     std::mutex mu;
@@ -176,7 +177,7 @@ void upload_request(xpr_server *s, Request *r)
         return p;
     };
     float *vol = (float *)take(4 * r->N);
-    char *images = take(s->esize * r->npix * r->S);
+    char *images = take(s->iesize * r->npix * r->S);
     xpr_projdata *pd = (xpr_projdata *)take(sizeof(xpr_projdata) * r->pd_sub.size());
     uint32_t *sums = (uint32_t *)take(4 * r->npix);
     void *ratio = take(s->esize * r->npix);
@@ -196,8 +197,8 @@ void upload_request(xpr_server *s, Request *r)
     stream_images(s, r, used, [&](int64_t i0, int64_t n, float *d) {
         for (int64_t j = i0; j < i0 + n; ++j) {
             const int64_t slot = (j % r->S) * r->Pc + j / r->S;
-            check_cuda(xpr::launch_preprocess(d + (j - i0) * WH, images + (size_t)slot * WH * s->esize,
-                                              s->opts.storage, WH, r->p.normalize ? 1 : 0, s->minmax,
+            check_cuda(xpr::launch_preprocess(d + (j - i0) * WH, images + (size_t)slot * WH * s->iesize,
+                                              s->opts.image_storage, WH, r->p.normalize ? 1 : 0, s->minmax,
                                               r->p.mlog ? 1 : 0, *s->di, s->io),
                        "preprocess");
         }
@@ -379,7 +380,7 @@ void compute_loop(xpr_server *s)
                                                         1, std::min(xpr::div_up(target, bricks), xpr::div_up(max_e, 4)));
         bool ok = true;
         for (Request *r : act) {
-            ok = ok && xpr::add_step_items(r->pp, r->step, splits, 16, s->opts.storage, &items);
+            ok = ok && xpr::add_step_items(r->pp, r->step, splits, 16, s->opts.image_storage, &items);
             pairs += r->N * (uint64_t)r->Pc;
         }
         const size_t fb = items.fwd.size() * sizeof(items.fwd[0]), eb = items.err.size() * sizeof(items.err[0]),
@@ -387,6 +388,7 @@ void compute_loop(xpr_server *s)
         const size_t eo = (fb + 255) & ~(size_t)255, bo = eo + ((eb + 255) & ~(size_t)255), need = bo + bb;
         cudaError_t e = cudaSuccess;
         const int h = (int)(tick & 1);
+        xpr::Range nvtx("xpr.serve_tick");
         if (ok && need > s->items_cap) {  // grow both buffers (rare): wait for the ticks in flight
             e = cudaStreamSynchronize(s->comp);
             for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
@@ -413,7 +415,7 @@ void compute_loop(xpr_server *s)
                                                 s->tickets, s->opts.arith, s->grid_fwd, s->comp);
             if (e == cudaSuccess)
                 e = xpr::launch_error_batched((const xpr::BatchErrItem *)(db + eo), (int)items.err.size(),
-                                              s->opts.storage, s->opts.storage, items.max_n, *s->di, s->comp);
+                                              s->opts.image_storage, s->opts.storage, items.max_n, *s->di, s->comp);
             if (e == cudaSuccess)
                 e = xpr::launch_backward_batched((const xpr::BatchBwdItem *)(db + bo), (int)items.bwd.size(),
                                                  items.bwd_units, s->tickets + 2, s->opts.arith, s->opts.storage, 16,
@@ -482,7 +484,7 @@ bool prepare_request(xpr_server *s, Request *r, std::string *msg)
     r->N = (uint64_t)r->go.vwidth * r->go.vheight * r->go.vwidth;
     r->npix = (uint64_t)r->Pc * r->W * r->H;
     auto al = [](uint64_t b) { return (b + 255) & ~255ull; };
-    r->bytes = al(4 * r->N) + al(s->esize * r->npix * r->S) + al(sizeof(xpr_projdata) * r->pd_sub.size()) +
+    r->bytes = al(4 * r->N) + al(s->iesize * r->npix * r->S) + al(sizeof(xpr_projdata) * r->pd_sub.size()) +
                al(4 * r->npix) + al(s->esize * r->npix);
     r->pairs = r->N * (uint64_t)r->Pc * (uint64_t)r->S * (uint64_t)r->p.it;
     return true;
@@ -538,11 +540,15 @@ int xpr_serve_create(xpr_ctx *ctx, const xpr_serve_opts *opts, xpr_server **out)
     if (o.arith != XPR_ARITH_STRICT && o.arith != XPR_ARITH_FAST) return fail(XPR_ERR_INVALID, "unknown arith");
     if (o.storage != XPR_F32 && o.storage != XPR_BF16 && o.storage != XPR_F16)
         return fail(XPR_ERR_INVALID, "unknown storage dtype");
+    if (!o.image_storage_set) o.image_storage = o.storage;
+    if (o.image_storage != XPR_F32 && o.image_storage != XPR_BF16 && o.image_storage != XPR_F16)
+        return fail(XPR_ERR_INVALID, "unknown image storage dtype");
     if (xpr::prepare_device_kernels() != cudaSuccess) return fail(XPR_ERR_CUDA, "xpr_serve_create: kernels");
     xpr_server *s = new xpr_server();
     s->ctx = ctx;
     s->di = di;
     s->esize = o.storage == XPR_F32 ? 4 : 2;
+    s->iesize = o.image_storage == XPR_F32 ? 4 : 2;
     s->t0 = std::chrono::steady_clock::now();
     if (o.mem_budget == 0) {
         uint64_t avail = 0;

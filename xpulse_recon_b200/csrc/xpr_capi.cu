@@ -203,6 +203,7 @@ int xpr_free_pinned(xpr_ctx *ctx, void *hptr)
 
 int xpr_upload(xpr_ctx *ctx, void *dst, const void *src, uint64_t bytes, void *stream)
 {
+    xpr::Range nvtx("xpr.upload");
     XPR_CHECK_CTX(ctx);
     if (!bytes) return XPR_OK;
     if (!dst || !src) return fail(XPR_ERR_INVALID, "NULL pointer");
@@ -212,6 +213,7 @@ int xpr_upload(xpr_ctx *ctx, void *dst, const void *src, uint64_t bytes, void *s
 
 int xpr_download(xpr_ctx *ctx, void *dst, const void *src, uint64_t bytes, void *stream)
 {
+    xpr::Range nvtx("xpr.download");
     XPR_CHECK_CTX(ctx);
     if (!bytes) return XPR_OK;
     if (!dst || !src) return fail(XPR_ERR_INVALID, "NULL pointer");
@@ -238,6 +240,7 @@ int xpr_synchronize(xpr_ctx *ctx, void *stream)
 int xpr_forward(xpr_ctx *ctx, const float *vol, uint32_t *sum, const xpr_projdata *pd, uint32_t n_pd,
                 const xpr_launch *L, void *stream)
 {
+    xpr::Range nvtx("xpr.forward");
     XPR_CHECK_CTX(ctx);
     if (!vol || !sum || !pd) return fail(XPR_ERR_INVALID, "NULL buffer");
     xpr::LaunchArgs a;
@@ -249,6 +252,7 @@ int xpr_forward(xpr_ctx *ctx, const float *vol, uint32_t *sum, const xpr_projdat
 int xpr_backward(xpr_ctx *ctx, float *vol, const void *ratio, int ratio_dtype, const xpr_projdata *pd, uint32_t n_pd,
                  const xpr_launch *L, void *stream)
 {
+    xpr::Range nvtx("xpr.backward");
     XPR_CHECK_CTX(ctx);
     if (!vol || !ratio || !pd) return fail(XPR_ERR_INVALID, "NULL buffer");
     if (!valid_dtype(ratio_dtype)) return fail(XPR_ERR_INVALID, "unknown ratio dtype %d", ratio_dtype);
@@ -262,6 +266,7 @@ int xpr_backward(xpr_ctx *ctx, float *vol, const void *ratio, int ratio_dtype, c
 int xpr_error(xpr_ctx *ctx, const void *images, int image_dtype, uint32_t *sum, void *ratio, int ratio_dtype,
               uint64_t n, float weight, int mode, int zero_sum, double *residual, void *stream)
 {
+    xpr::Range nvtx("xpr.error");
     XPR_CHECK_CTX(ctx);
     if (!images || !sum || !ratio) return fail(XPR_ERR_INVALID, "NULL buffer");
     if (!valid_dtype(image_dtype) || !valid_dtype(ratio_dtype)) return fail(XPR_ERR_INVALID, "unknown dtype");
@@ -274,6 +279,7 @@ int xpr_error(xpr_ctx *ctx, const void *images, int image_dtype, uint32_t *sum, 
 
 int xpr_preprocess_minmax(xpr_ctx *ctx, const float *images, uint64_t n, float *minmax, void *stream)
 {
+    xpr::Range nvtx("xpr.preprocess_minmax");
     XPR_CHECK_CTX(ctx);
     if (!minmax || (n && !images)) return fail(XPR_ERR_INVALID, "NULL buffer");
     cudaError_t e = xpr::launch_minmax(images, n, minmax, ctx->dev, as_stream(stream));
@@ -283,6 +289,7 @@ int xpr_preprocess_minmax(xpr_ctx *ctx, const float *images, uint64_t n, float *
 int xpr_preprocess_apply(xpr_ctx *ctx, const float *images, void *out, int out_dtype, uint64_t n, int normalize,
                          const float *minmax, int mlog, void *stream)
 {
+    xpr::Range nvtx("xpr.preprocess");
     XPR_CHECK_CTX(ctx);
     if (n && (!images || !out)) return fail(XPR_ERR_INVALID, "NULL buffer");
     if (normalize && !minmax) return fail(XPR_ERR_INVALID, "normalize needs minmax");
@@ -296,6 +303,7 @@ int xpr_subiteration(xpr_ctx *ctx, float *vol, uint32_t *sum, const void *images
                      int ratio_dtype, const xpr_projdata *pd, uint32_t n_pd, const xpr_launch *L, float weight,
                      int first, double *residual, void *stream)
 {
+    xpr::Range nvtx("xpr.subiteration");
     XPR_CHECK_CTX(ctx);
     if (!vol || !sum || !images || !ratio || !pd) return fail(XPR_ERR_INVALID, "NULL buffer");
     if (!valid_dtype(image_dtype) || !valid_dtype(ratio_dtype)) return fail(XPR_ERR_INVALID, "unknown dtype");

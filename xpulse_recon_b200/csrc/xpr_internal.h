@@ -4,10 +4,21 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/xpr.h"
 
 namespace xpr {
+
+// A named NVTX range around a phase (forward, error, backward, upload, download,
+// preprocessing, a sub-iteration) for a profiler's timeline; it marks the host-side
+// enqueue of asynchronous work.  Without a profiler attached push / pop cost a few ns.
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
 
 // Validated launch description shared by the forward / backward launchers.
 struct LaunchArgs {

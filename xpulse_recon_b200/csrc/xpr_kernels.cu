@@ -299,6 +299,48 @@ __device__ __forceinline__ uint64_t addrz2(uint64_t a, uint64_t b)
     asm("add.rz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
     return d;
 }
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// Correctly rounded quotient a / b (IEEE round to nearest) for a divisor shared by many
+// dividends, from y = RN(1/b) and ylo = RN(RN(1 - b*y) * y), computed once per divisor.
+// y + ylo approximates 1/b to about 2^-47, so q0 = RN(a*y + RN(a*ylo)) lies within one ulp
+// of a/b; the residual a - b*q0 is then exact (one fma), and RN(q0 + r*y) is the correctly
+// rounded quotient (Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  The argument needs a, b, the
+// quotient and the residual away from overflow; callers screen |b| in [2^-60, 2^60] and
+// |a| < 2^102.  A quotient in the subnormal range may be off in its last bits, which no
+// pixel decision can see (|a/b| < 2^-100 rounds to pixel 0 either way).
+__device__ __forceinline__ float div_exact(float a, float nb, float y, float ylo)  // nb = -b
+{
+    const float q0 = __fmaf_rn(a, y, __fmul_rn(a, ylo));
+    return __fmaf_rn(__fmaf_rn(nb, q0, a), y, q0);
+}
+// the same for two dividends (register pair) and one divisor
+__device__ __forceinline__ uint64_t div_exact2(uint64_t a, uint64_t nb, uint64_t y, uint64_t ylo)
+{
+    const uint64_t q0 = fma2(a, y, mul2(a, ylo));
+    return fma2(fma2(nb, q0, a), y, q0);
+}
+// Pixel of a STRICT coordinate q (the reference rounds half away from zero, then
+// subtracts nothing (u) or an integer row offset first (v)): bits(RZ(RZ(q + 1/2) + 2^23))
+// - base with base = 2^23's bits + off + lo is the buffer pixel minus lo for every q
+// whose pixel can be in [lo, lo + n) (n <= 2^22), and >= 2^22 as unsigned otherwise,
+// except q = off - 1/2 exactly (the reference gives -1 there, this gives 0).  For
+// in-bounds pixels q - off is exact (|q - off| <= |q| and both are on q's ulp grid),
+// and floor(RZ(x)) = floor(x) for x >= 0 because the integers below 2^24 are floats.
+__device__ __forceinline__ uint64_t pix_bits2(uint64_t q, uint64_t half, uint64_t magic)
+{
+    return addrz2(addrz2(q, half), magic);
+}
+__device__ __forceinline__ uint32_t pix_bits(float q)
+{
+    return __float_as_uint(__fadd_rz(__fadd_rz(q, 0.5f), 8388608.0f));
+}
 // y position of layer k of a column, from its pairs or from a plain array
 template <int N>
 __device__ __forceinline__ float ypos(const uint64_t (&py2)[N], int k)
@@ -486,6 +528,80 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
     return 1;
 }
 
+// y positions {py[2m], py[2m + 1]} of a column as a register pair
+template <int N>
+__device__ __forceinline__ uint64_t ypair(const float (&py)[N], int m)
+{
+    return f2pack(py[2 * m], py[2 * m + 1]);
+}
+template <int N>
+__device__ __forceinline__ uint64_t ypair(const uint64_t (&py2)[N], int m)
+{
+    return py2[m];
+}
+
+// STRICT-contract walk of an untilted column (same calls and return value as walk_fast),
+// bit-identical to the reference's per-voxel division: n_v = ((c.x*px + c.y*py) + c.z*pz)
+// + c.w in the reference's order, v = n_v / n_w by div_exact with the column's n_w, and
+// the pixel by pix_bits2.  Returns -1, without calling f, when some lane's column is
+// outside div_exact's screened range (the caller then divides per voxel).
+template <int LEN, typename PY, typename F>
+__device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a, float nu, float nw, float Pv,
+                                          float Rv, const PY &py2, F &&f)
+{
+    static_assert(LEN % 2 == 0, "columns are walked two voxels at a time");
+    const float4 cv = M.cv;
+    const int4 rc = M.rect;
+    const uint4 tgt = M.tgt;
+    const uint32_t pitch = tgt.x;
+    // every partial sum of n_v is below the sum of its terms' magnitudes (NaN / inf fail)
+    const float ay = fmaxf(fabsf(ypos(py2, 0)), fabsf(ypos(py2, LEN - 1)));
+    const float bound = __fadd_rn(__fadd_rn(fabsf(Pv), fabsf(Rv)), __fadd_rn(fabsf(cv.w), __fmul_rn(fabsf(cv.y), ay)));
+    const float aw = fabsf(nw);
+    const bool safe = aw >= 0x1p-60f && aw <= 0x1p60f && bound < 0x1p100f && fabsf(nu) < 0x1p100f;
+    if (!__all_sync(0xffffffffu, safe)) return -1;
+    const float y = __frcp_rn(nw);
+    const float ylo = __fmul_rn(__fmaf_rn(-nw, y, 1.0f), y);
+    const float qu = div_exact(nu, -nw, y, ylo);
+    const uint32_t du = pix_bits(qu) - (kMagic + (uint32_t)rc.x);
+    const uint64_t cvy = f2pack(cv.y, cv.y), P2 = f2pack(Pv, Pv), R2 = f2pack(Rv, Rv), W2 = f2pack(cv.w, cv.w);
+    const uint64_t Y2 = f2pack(y, y), YL2 = f2pack(ylo, ylo), NB2 = f2pack(-nw, -nw);
+    const uint64_t half = f2pack(0.5f, 0.5f), magic = f2pack(8388608.0f, 8388608.0f);
+    const uint32_t base_v = kMagic + (uint32_t)a.row_off_f + (uint32_t)rc.z;
+    auto qv = [&](int m) {
+        const uint64_t nv = add2(add2(add2(P2, mul2(ypair(py2, m), cvy)), R2), W2);
+        return div_exact2(nv, NB2, Y2, YL2);
+    };
+    if (M.flags.w) {
+        // inside: every pixel is in the rectangle, idx = bits * pitch + K (mod 2^32)
+        const uint32_t K = du + tgt.y - base_v * pitch;
+#pragma unroll
+        for (int k = 0; k < LEN; k += 2) {
+            uint32_t b0, b1;
+            u2unpack(pix_bits2(qv(k >> 1), half, magic), b0, b1);
+            f(std::true_type{}, k, true, b0 * pitch + K);
+            f(std::true_type{}, k + 1, true, b1 * pitch + K);
+        }
+        return 2;
+    }
+    const bool in_u = (du < (uint32_t)rc.y) && (qu != -0.5f);
+    if (!__any_sync(0xffffffffu, in_u)) return 0;
+    const uint32_t K = du + tgt.y;
+    const float ex = __fsub_rn(a.row_off_f, 0.5f);  // pix_bits2's one exception
+#pragma unroll
+    for (int k = 0; k < LEN; k += 2) {
+        const uint64_t q = qv(k >> 1);
+        uint32_t b0, b1;
+        float q0, q1;
+        u2unpack(pix_bits2(q, half, magic), b0, b1);
+        f2unpack(q, q0, q1);
+        const uint32_t dv0 = b0 - base_v, dv1 = b1 - base_v;
+        f(std::false_type{}, k, in_u && (dv0 < (uint32_t)rc.w) && (q0 != ex), dv0 * pitch + K);
+        f(std::false_type{}, k + 1, in_u && (dv1 < (uint32_t)rc.w) && (q1 != ex), dv1 * pitch + K);
+    }
+    return 1;
+}
+
 // Column walker.  For the voxel column (ax, az) and y-positions py[0..LEN) (in pairs
 // py2[m] = {py[2m], py[2m + 1]}), calls
 // f(inside, k, in, idx) with idx the target index of ProjMeta.  Untilted projections
@@ -514,6 +630,8 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
             // column invariants
             const float nu = num_strict(cu, px, 0.0f, pz);
             const float nw = num_strict(cw, px, 0.0f, pz);
+            const int w = walk_exact<LEN>(M, a, nu, nw, __fmul_rn(cv.x, px), __fmul_rn(cv.z, pz), py2, f);
+            if (w >= 0) return w;
             const uint32_t du = (uint32_t)(__float2int_rz(roundf(__fdiv_rn(nu, nw))) - rc.x);
             const bool in_u = du < (uint32_t)rc.y;
             if (!__any_sync(0xffffffffu, in_u)) return 0;

@@ -19,7 +19,7 @@ QUEUED, ACTIVE, DONE, FAILED = 0, 1, 2, 3
 
 class ServeOpts(C.Structure):
     _fields_ = [("arith", C.c_int32), ("storage", C.c_int32), ("mem_budget", C.c_uint64),
-                ("max_active", C.c_uint32)]
+                ("max_active", C.c_uint32), ("image_storage_set", C.c_int32), ("image_storage", C.c_int32)]
 
 
 class RequestInfo(C.Structure):
@@ -66,13 +66,15 @@ def grid_of(params: dict, width: int, height: int) -> tuple:
 class Server:
     """xpr_server handle; keeps every submitted request's raw images and output alive."""
 
-    def __init__(self, ctx, arith: int = _lib.FAST, storage: int = _lib.F32, mem_budget: int = 0,
-                 max_active: int = 0):
+    def __init__(self, ctx, arith: int = _lib.STRICT, storage: int = _lib.F32, mem_budget: int = 0,
+                 max_active: int = 0, image_storage: int = None):
+        """storage: the ratios' dtype, and the images' unless image_storage is given."""
         L = lib()
         _signatures(L)
         self.ctx = ctx
         h = C.c_void_p()
-        o = ServeOpts(arith, storage, mem_budget, max_active)
+        o = ServeOpts(arith, storage, mem_budget, max_active, int(image_storage is not None),
+                      storage if image_storage is None else image_storage)
         check(L.xpr_serve_create(ctx.handle, C.byref(o), C.byref(h)), "xpr_serve_create")
         self.handle = h
         self._keep = {}
