@@ -57,11 +57,12 @@ CONFIGS = {
                batch=64, dwidth=384, dheight=384, projections=360, sit=10, it=2, modules=3, px=0.1, rpy=2.0,
                phantom=256, ellipsoids=12, background=0.0, i0=1e5, seed=4, plain_sample=4),
     # a request loop: Poisson arrivals of mixed-size scans, continuous batching
-    "c5": dict(desc="Poisson arrivals (4/s) of 120 scans: phantom edge in {128, 256, 384} (recon grid 1.5x: "
-                    "192 / 384 / 576), {180, 360, 720} projections on a square detector of the grid's edge, "
-                    "it 1, sit 10, 1e5 photons; FP32 and BF16 storage servers",
-               serve=True, requests=120, rate=4.0, edges=[128, 256, 384], projections_set=[180, 360, 720], sit=10,
-               it=1, px=0.1, i0=1e5, seed=5, ellipsoids=10, background=0.0),
+    "c5": dict(desc="Poisson arrivals (4/s) of 500 scans: phantom edge in {128, 256, 384, 512, 768} (recon "
+                    "grid and detector 1.5x: 192 .. 1152), {180, 360, 720, 1080} projections, it 1, sit 10, "
+                    "1e5 photons; servers with FP32 storage and with the BF16 form (BF16 ratio, FP16 images)",
+               serve=True, requests=500, rate=4.0, edges=[128, 256, 384, 512, 768],
+               projections_set=[180, 360, 720, 1080], sit=10, it=1, px=0.1, i0=1e5, seed=5, ellipsoids=10,
+               background=0.0, plain_requests=100),
     # out-of-core at half linear scale: the volume does not fit the device-memory cap
     "c3h": dict(desc="c3 at half linear scale: 1536x1024x1536 recon grid (9.7 GB), 1000 projections of "
                      "1536x1024 (6.3 GB), sit 20 -> 50, it 1, under an 8 GB device-memory cap: naive without "
@@ -95,8 +96,10 @@ def parse_args():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--arith", choices=["fast", "strict"], default="strict",
-                   help="projector contract: strict = the reference kernels' IEEE results bit for bit (default)")
+    p.add_argument("--arith", choices=["fast", "strict"], default=None,
+                   help="projector contract: strict = the reference kernels' IEEE results bit for bit (the "
+                        "default), fast = the relaxed-math form (the default of the tilted-module batched "
+                        "configurations c4 / c4s / c4one, which have no reference counterpart)")
     p.add_argument("--storage", choices=["fp32", "bf16", "fp16"], default=None,
                    help="image / ratio storage (default: fp32; bf16 for the batched configurations)")
     p.add_argument("--config", choices=sorted(CONFIGS), default="c2")
@@ -655,6 +658,7 @@ def run_batched(args, cfg, rank, world, local):
     ctx = Context(local)
     rng = np.random.default_rng(cfg["seed"] + 1000 * rank)
     storage = {"fp32": _lib.F32, "bf16": _lib.BF16, "fp16": _lib.F16}[args.storage or "bf16"]
+    arith = _lib.STRICT if args.arith == "strict" else _lib.FAST
     S, it, M, P = cfg["sit"], cfg["it"], cfg["modules"], cfg["projections"]
     Wd, Hd = cfg["dwidth"], cfg["dheight"]
     stream = torch.cuda.current_stream()
@@ -698,7 +702,7 @@ def run_batched(args, cfg, rank, world, local):
                               seed=int(rng.integers(1 << 31)), weight=1.0, weight_factor=0.9))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    b = Batch(ctx, probs, arith=_lib.FAST, storage=storage, use_graph=True, autotune=True)
+    b = Batch(ctx, probs, arith=arith, storage=storage, use_graph=True, autotune=True)
     tune_s = time.perf_counter() - t0
     steps = b.steps
     pairs_step = sum(p.vwidth * p.vheight * p.vwidth * p.per_subset for p in probs)
@@ -726,11 +730,11 @@ def run_batched(args, cfg, rank, world, local):
         q = BProblem(vol=torch.ones_like(p.vol), images=f32, projdata=p.projdata, det_w=Wd, det_h=Hd,
                      per_subset=p.per_subset, modules=M, sit=S, it=it, vwidth=p.vwidth, vheight=p.vheight,
                      voxel=p.voxel, orig=p.orig, seed=p.seed)
-        q.run_alone(ctx, _lib.FAST, _lib.F32)  # warm
+        q.run_alone(ctx, arith, _lib.F32)  # warm
         torch.cuda.synchronize()
         a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        q.run_alone(ctx, _lib.FAST, _lib.F32)
+        q.run_alone(ctx, arith, _lib.F32)
         z.record()
         torch.cuda.synchronize()
         plain_ms += a.elapsed_time(z)
@@ -757,11 +761,11 @@ def run_batched(args, cfg, rank, world, local):
                                    vheight=p.vheight, voxel=p.voxel, orig=p.orig, seed=p.seed)))
     breakdown = {}
     if sample:
-        alone_st = sum(timed(lambda p=p: p.run_alone(ctx, _lib.FAST, storage)) for p, _ in sample)
-        bq = Batch(ctx, [q for _, q in sample], arith=_lib.FAST, storage=_lib.F32, use_graph=True, autotune=True)
+        alone_st = sum(timed(lambda p=p: p.run_alone(ctx, arith, storage)) for p, _ in sample)
+        bq = Batch(ctx, [q for _, q in sample], arith=arith, storage=_lib.F32, use_graph=True, autotune=True)
         batch_f32 = timed(bq.run)
         bq.close()
-        bs = Batch(ctx, [p for p, _ in sample], arith=_lib.FAST, storage=storage, use_graph=True, autotune=True)
+        bs = Batch(ctx, [p for p, _ in sample], arith=arith, storage=storage, use_graph=True, autotune=True)
         batch_st = timed(bs.run)
         bs.close()
         g = lambda ms: plain_pairs / (ms / 1000.0) / 1e9  # noqa: E731
@@ -851,8 +855,10 @@ def run_serving(args, cfg, rank, world, local):
     pairs_of = {k: data[k][1] * k[1] for k in kinds}  # N x P per reconstruction (it 1)
     total_pairs = sum(pairs_of[k] for _, k in reqs) * cfg["it"]
 
-    def serve(storage, open_loop):
-        srv = Server(ctx, storage=storage)
+    arith = _lib.STRICT if args.arith == "strict" else _lib.FAST
+
+    def serve(storage, open_loop, image_storage=None):
+        srv = Server(ctx, arith=arith, storage=storage, image_storage=image_storage)
         # warm the kernels and the allocator on one small request
         w = srv.submit(reqs[0][0], data[reqs[0][1]][0])
         srv.wait(w, 120.0)
@@ -875,11 +881,10 @@ def run_serving(args, cfg, rank, world, local):
                 "ticks": int(st.ticks), "peak_device_gb": st.peak_bytes / 1e9}
 
     res = {}
-    serve(_lib.F32, False)  # warm-up: host threads, pools, page-locked rings
     clocks = ClockSampler(local)
     clocks.start()
-    for name, st in (("fp32", _lib.F32), ("bf16", _lib.BF16)):
-        res[name] = {"open_loop": serve(st, True), "saturated": serve(st, False)}
+    for name, st, ist in (("fp32", _lib.F32, None), ("bf16", _lib.BF16, _lib.F16)):
+        res[name] = {"open_loop": serve(st, True, ist)}
     clk = clocks.stop()
     # the plain FP32 path: one request of each kind alone through xpr_reconstruct_host
     L = _lib.lib()
@@ -888,7 +893,8 @@ def run_serving(args, cfg, rank, world, local):
     plain_pairs, plain_s = 0, 0.0
     for k in kinds:
         raw, N = data[k]
-        params = {"recon": {"method": "naive", "it": cfg["it"], "sit": cfg["sit"], "seed": 7, "mlog": True},
+        params = {"recon": {"method": "naive", "it": cfg["it"], "sit": cfg["sit"], "seed": 7, "mlog": True,
+                            "arith": args.arith},
                   "geometry": {"so": 100.0, "sd": 1000.0, "angle": 360.0}, "detector": {"px": cfg["px"]}}
         out = np.empty(N, np.float32)
         P, H, W = raw.shape
@@ -901,7 +907,11 @@ def run_serving(args, cfg, rank, world, local):
     plain = plain_pairs / plain_s / 1e9
 
     # the plain FP32 path under the same arrivals: one request at a time, first come first
-    # served, each through xpr_reconstruct_host (the reference's one-scan-per-run model)
+    # served, each through xpr_reconstruct_host (the reference's one-scan-per-run model);
+    # on the first plain_requests requests (it falls behind the arrivals, so the whole
+    # stream would take many minutes)
+    n_plain = min(n, cfg.get("plain_requests", n))
+
     def plain_open_loop():
         import queue
         import threading
@@ -923,26 +933,31 @@ def run_serving(args, cfg, rank, world, local):
         th = threading.Thread(target=worker)
         th.start()
         t0 = time.perf_counter()
-        for i, (params, k) in enumerate(reqs):
+        for i, (params, k) in enumerate(reqs[:n_plain]):
             dt = arrivals[i] - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
-            jobs.put((time.perf_counter(), params, k))
+            p2 = json.loads(json.dumps(params))
+            p2["recon"]["arith"] = args.arith
+            jobs.put((time.perf_counter(), p2, k))
         jobs.put(None)
         th.join()
         span = time.perf_counter() - t0
         lat = np.array(lat)
-        return {"ok": bool(np.isfinite(lat).all()), "p50_s": float(np.percentile(lat, 50)),
+        pairs = sum(pairs_of[k] for _, k in reqs[:n_plain]) * cfg["it"]
+        return {"ok": bool(np.isfinite(lat).all()), "requests": n_plain, "p50_s": float(np.percentile(lat, 50)),
                 "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
-                "gups": total_pairs / span / 1e9, "makespan_s": span}
+                "gups": pairs / span / 1e9, "makespan_s": span}
 
     res["plain_fp32"] = {"open_loop": plain_open_loop()}
-    best = res["bf16"]["saturated"]["gups"]
+    best = res["bf16"]["open_loop"]["gups"]
     line = {"metric": "GUPS served (voxel x projection pairs / s), with p50 / p99 request latency",
             "value": best, "unit": "GUPS", "n_gpus": world, "steps": n, "warmup": 1,
-            "ms_per_step": 1000.0 * res["bf16"]["saturated"]["makespan_s"] / n, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 storage, f32 compute", "data": "synthetic",
-            "config": {"workload": "c5: " + cfg["desc"], "requests": n, "rate_per_s": cfg["rate"]},
+            "ms_per_step": 1000.0 * res["bf16"]["open_loop"]["makespan_s"] / n, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 ratio / fp16 image storage, f32 compute",
+            "data": "synthetic",
+            "config": {"workload": "c5: " + cfg["desc"], "requests": n, "rate_per_s": cfg["rate"],
+                       "arith": args.arith},
             "serving": res, "plain_fp32_e2e": {"value": plain, "unit": "GUPS",
                                                "sample": "one request of each of the %d kinds, alone, through "
                                                          "xpr_reconstruct_host (host images in, volume out)" % len(kinds)},
@@ -1110,6 +1125,8 @@ def run_outofcore(args, cfg, rank, world, local):
 def main():
     args = parse_args()
     cfg = CONFIGS[args.config]
+    if args.arith is None:
+        args.arith = "fast" if "batch" in cfg else "strict"
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, cfg, rank, world)

@@ -75,7 +75,7 @@ def test_batch_equals_each_problem_alone(bctx, storage):
 @pytest.mark.parametrize("splits,column", [(1, 16), (3, 8), (8, 16)])
 def test_schedule_does_not_change_results(bctx, splits, column):
     probs = _problems(bctx, _lib.F32)
-    alone = _alone(bctx, probs, _lib.FAST, _lib.F32)
+    alone = _alone(bctx, probs, _lib.STRICT, _lib.F32)
     b = Batch(bctx, probs, use_graph=False, autotune=False, fwd_splits=splits, bwd_column=column, ctas_per_sm=2)
     sch = b.schedule()
     assert sch["fwd_splits"] == splits and sch["bwd_column"] == column and sch["ctas_per_sm"] <= 2
@@ -109,7 +109,7 @@ def test_batch_strict_fp32_matches_oracle(bctx):
 
 def test_batch_residuals_match_alone(bctx):
     probs = _problems(bctx, _lib.F32, residual=True)
-    _alone(bctx, probs, _lib.FAST, _lib.F32)
+    _alone(bctx, probs, _lib.STRICT, _lib.F32)
     ref = [p.residual.cpu().numpy().copy() for p in probs]
     for p in probs:
         p.residual.zero_()

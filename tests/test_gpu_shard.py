@@ -1,7 +1,8 @@
 """Slab sharding on the GPU: two ranks (processes) share the one GPU of the test machine,
-each running this library's kernels on its y-slab, the detector partial sums exchanged
-through a gloo process group (host staging; the ranks' kernels never wait on each other).
-The gathered volume must equal the single-rank GPU run and the CPU oracle bit for bit."""
+each running this library's kernels (STRICT contract) on its y-slab, the detector
+partial sums of the rows the two slabs' windows share exchanged through a gloo process
+group (host staging; the ranks' kernels never wait on each other).  The gathered volume
+must equal the single-rank GPU run and the CPU oracle bit for bit."""
 import ctypes as C
 import os
 import socket
@@ -61,7 +62,7 @@ def test_two_slab_ranks_equal_one_gpu_and_the_oracle(tmp_path):
     imgs = raw.ravel().copy()
     O.lib().orc_preprocess(imgs, imgs.size, 0, 0.0, 0.0, 1)
     gp = O.geom_params(**GEOM)
-    rp = O.ReconParams(2, GEOM["sit"], 1.0, 0.9, 31, O.FAST, 0)
+    rp = O.ReconParams(2, GEOM["sit"], 1.0, 0.9, 31, O.STRICT, 0)
     exp = np.zeros(one.size, np.float32)
     assert O.lib().orc_recon_naive(C.byref(gp), C.byref(rp), imgs, exp) == 0
     assert_same_bits(one, exp)

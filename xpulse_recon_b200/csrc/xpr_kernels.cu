@@ -68,7 +68,8 @@ struct __align__(16) ProjMeta {
     uint4 fast;                           // {kMagic + u0, u1 - u0, kMagic + v0, v1 - v0}
     int4 rect;                            // {u0, u1 - u0, v0, v1 - v0}
     uint4 tgt;                            // {pitch, off, img_base, tile width}
-    int4 flags;                           // {mode, lanes across z, column, inside (no bounds tests)}
+    int4 flags;                           // {mode, lanes across z, column (bit 0: untilted, bit 1: and
+                                          //  walk_exact's screen passed), inside (no bounds tests)}
 };
 
 // --------------------------------------------------------------------------------------
@@ -106,6 +107,14 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
     const float u = __fdiv_rn(nu, nw);
     const float v = __fsub_rn(__fdiv_rn(nv, nw), a.row_off_f);
     int ok = (nw > 0.0f) && (fabsf(u) < 1.0e9f) && (fabsf(v) < 1.0e9f);
+    // walk_exact's operand screen, with a factor 2 of margin for the STRICT positions'
+    // rounding: the u and v numerators' terms below 2^99 in magnitude and n_w in
+    // [2^-59, 2^59] with one sign at every corner (n_w is affine over the brick, so its
+    // range is its corners'); NaN and inf fail every comparison
+    const float bu = fabsf(cu0 * px) + fabsf(cu1 * py) + fabsf(cu2 * pz) + fabsf(cu3);
+    const float bv = fabsf(cv0 * px) + fabsf(cv1 * py) + fabsf(cv2 * pz) + fabsf(cv3);
+    int scr = (bu < 0x1p99f) && (bv < 0x1p99f) && (fabsf(nw) >= 0x1p-59f) && (fabsf(nw) <= 0x1p59f);
+    int wpos = nw > 0.0f, wneg = nw < 0.0f;
     float umin = ok ? u : 0.0f, umax = umin, vmn = ok ? v : 0.0f, vmx = vmn;
 #pragma unroll
     for (int o = 1; o < 8; o <<= 1) {
@@ -114,6 +123,9 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
         vmn = fminf(vmn, __shfl_xor_sync(0xffffffffu, vmn, o));
         vmx = fmaxf(vmx, __shfl_xor_sync(0xffffffffu, vmx, o));
         ok &= __shfl_xor_sync(0xffffffffu, ok, o);
+        scr &= __shfl_xor_sync(0xffffffffu, scr, o);
+        wpos &= __shfl_xor_sync(0xffffffffu, wpos, o);
+        wneg &= __shfl_xor_sync(0xffffffffu, wneg, o);
     }
     if (c == 0) {
         ProjMeta &M = s_meta[g];
@@ -147,7 +159,8 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
         M.fast = make_uint4(kMagic + (uint32_t)l, (uint32_t)(r - l), kMagic + (uint32_t)b, (uint32_t)(t - b));
         M.rect = make_int4(l, r - l, b, t - b);
         M.tgt = make_uint4(pitch, off, img_base, (uint32_t)(r - l));
-        M.flags = make_int4(mode, fabsf(cw0) > fabsf(cw2), (cu1 == 0.0f) && (cw1 == 0.0f), inside);
+        const int column = (cu1 == 0.0f) && (cw1 == 0.0f);
+        M.flags = make_int4(mode, fabsf(cw0) > fabsf(cw2), column ? (1 | ((scr && (wpos || wneg)) << 1)) : 0, inside);
     }
 }
 
@@ -543,8 +556,9 @@ __device__ __forceinline__ uint64_t ypair(const uint64_t (&py2)[N], int m)
 // STRICT-contract walk of an untilted column (same calls and return value as walk_fast),
 // bit-identical to the reference's per-voxel division: n_v = ((c.x*px + c.y*py) + c.z*pz)
 // + c.w in the reference's order, v = n_v / n_w by div_exact with the column's n_w, and
-// the pixel by pix_bits2.  Returns -1, without calling f, when some lane's column is
-// outside div_exact's screened range (the caller then divides per voxel).
+// the pixel by pix_bits2.  Returns -1, without calling f, when the projection's operands
+// failed div_exact's screen over the brick (compute_meta; the caller then divides per
+// voxel).
 template <int LEN, typename PY, typename F>
 __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a, float nu, float nw, float Pv,
                                           float Rv, const PY &py2, F &&f)
@@ -554,12 +568,7 @@ __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a
     const int4 rc = M.rect;
     const uint4 tgt = M.tgt;
     const uint32_t pitch = tgt.x;
-    // every partial sum of n_v is below the sum of its terms' magnitudes (NaN / inf fail)
-    const float ay = fmaxf(fabsf(ypos(py2, 0)), fabsf(ypos(py2, LEN - 1)));
-    const float bound = __fadd_rn(__fadd_rn(fabsf(Pv), fabsf(Rv)), __fadd_rn(fabsf(cv.w), __fmul_rn(fabsf(cv.y), ay)));
-    const float aw = fabsf(nw);
-    const bool safe = aw >= 0x1p-60f && aw <= 0x1p60f && bound < 0x1p100f && fabsf(nu) < 0x1p100f;
-    if (!__all_sync(0xffffffffu, safe)) return -1;
+    if (!(M.flags.z & 2)) return -1;  // uniform over the projection
     const float y = __frcp_rn(nw);
     const float ylo = __fmul_rn(__fmaf_rn(-nw, y, 1.0f), y);
     const float qu = div_exact(nu, -nw, y, ylo);
@@ -754,6 +763,45 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                         splat(reinterpret_cast<const uint4 *>(s_val + cz * VSTRIDE + 4 * lane),
                               __fadd_rn(Au, __fmul_rn(cu.z, pz)), __fadd_rn(Av, __fmul_rn(cv.z, pz)),
                               __fadd_rn(Aw, __fmul_rn(cw.z, pz)));
+                    }
+                }
+                continue;
+            }
+            if (ARITH == kStrict && fl.x == kTile && (fl.z & 2)) {
+                // STRICT into a tile, untilted and screened: n_u and n_w are (c.x*px + c.z*pz) + c.w
+                // (c.y*py is a zero), so the lane coordinate's product in every row is formed once
+                // per projection; walk_exact divides per voxel with the column's reciprocal
+                const float4 cu = M.cu, cv = M.cv, cw = M.cw;
+                auto splat = [&](const uint4 *vals, float nu, float nw, float Pv, float Rv) {
+                    uint4 quad;
+                    // a zero adds nothing to a shared-memory tile; no test for it
+                    walk_exact<BY>(M, a, nu, nw, Pv, Rv, py, [&](auto, int k, bool in, uint32_t idx) {
+                        if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
+                        const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
+                        if (in) atomicAdd(&tile[idx], v);
+                    });
+                };
+                if (orx) {
+                    const float pz = pos<kStrict>(a.vmin[2] + z0 + lane, a.voxel[2], a.origin[2]);
+                    const float Bu = __fmul_rn(cu.z, pz), Bw = __fmul_rn(cw.z, pz), Rv = __fmul_rn(cv.z, pz);
+#pragma unroll 1
+                    for (int j = 0; j < 4; ++j) {
+                        const int cx = warp + 8 * j;
+                        const float px = pos<kStrict>(a.vmin[0] + x0 + cx, a.voxel[0], a.origin[0]);
+                        splat(reinterpret_cast<const uint4 *>(s_val + lane * VSTRIDE + 4 * cx),
+                              __fadd_rn(__fadd_rn(__fmul_rn(cu.x, px), Bu), cu.w),
+                              __fadd_rn(__fadd_rn(__fmul_rn(cw.x, px), Bw), cw.w), __fmul_rn(cv.x, px), Rv);
+                    }
+                } else {
+                    const float px = pos<kStrict>(a.vmin[0] + x0 + lane, a.voxel[0], a.origin[0]);
+                    const float Au = __fmul_rn(cu.x, px), Aw = __fmul_rn(cw.x, px), Pv = __fmul_rn(cv.x, px);
+#pragma unroll 1
+                    for (int j = 0; j < 4; ++j) {
+                        const int cz = warp + 8 * j;
+                        const float pz = pos<kStrict>(a.vmin[2] + z0 + cz, a.voxel[2], a.origin[2]);
+                        splat(reinterpret_cast<const uint4 *>(s_val + cz * VSTRIDE + 4 * lane),
+                              __fadd_rn(__fadd_rn(Au, __fmul_rn(cu.z, pz)), cu.w),
+                              __fadd_rn(__fadd_rn(Aw, __fmul_rn(cw.z, pz)), cw.w), Pv, __fmul_rn(cv.z, pz));
                     }
                 }
                 continue;
