@@ -219,3 +219,23 @@ def test_culling_matches_oracle(L, name):
             assert n.value == m
             np.testing.assert_array_equal(a1[:m], b1[:m])
             np.testing.assert_array_equal(a2[:m], b2[:m])
+
+
+def test_strict_walk_division_and_pixel_rule_on_the_cpu(tmp_path):
+    """The STRICT column walk divides by a column's n_w with a reciprocal, its residual and
+    one Markstein correction, and rounds half away from zero with two round-toward-zero
+    adds (xpr_kernels.cu: div_exact, pix_bits2).  The same operations in C on the host
+    (hardware fma, IEEE division) must give the IEEE quotient and the reference's pixel
+    on 10^8 operand pairs (half of them at rounding midpoints) and 2 x 10^7 pixel
+    decisions around half-integer borders; the GPU parity tests then show the kernels
+    equal to the reference bit for bit."""
+    src = os.path.join(os.path.dirname(os.path.abspath(__file__)), "exact_div_check.c")
+    exe = str(tmp_path / "exact_div_check")
+    r = subprocess.run(["gcc", "-O2", "-mfma", "-fopenmp", "-ffp-contract=off", "-frounding-math", "-o", exe, src,
+                        "-lm"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([exe, "2000", "50000"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    res = {line.split()[0]: (int(line.split()[1]), int(line.split()[2])) for line in out.stdout.splitlines()}
+    assert res["division"][0] == 2000 * 50000 and res["division"][1] == 0, res
+    assert res["pixel"][0] == 20000000 and res["pixel"][1] == 0, res
