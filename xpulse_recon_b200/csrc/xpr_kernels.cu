@@ -70,13 +70,14 @@ struct __align__(16) ProjMeta {
     uint4 tgt;                            // {pitch, off, img_base, tile width}
     int4 flags;                           // {mode, lanes across z, column (bit 0: untilted, bit 1: and
                                           //  walk_exact's screen passed), inside (no bounds tests)}
+    float T[16];                          // STRICT: c_v.y * py of the brick's layers (the reference's rounding)
 };
 
 // --------------------------------------------------------------------------------------
 // per-projection metadata: one group of G entries, computed by warp 0
 // lane = g * 8 + corner of the brick [x0, x0+ex) x [y0, y0+ey) x [z0, z0+ez)
 // --------------------------------------------------------------------------------------
-template <bool LIST, bool GATHER>
+template <int ARITH, bool LIST, bool GATHER>
 __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdata *__restrict__ pd,
                                              const LaunchArgs &a, int e0, int e_end, int bx0, int by0, int bz0,
                                              int ex, int ey, int ez, int lane)
@@ -101,6 +102,18 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
     const float px = __fmaf_rn((float)ix, a.voxel[0], a.origin[0]);
     const float py = __fmaf_rn((float)iy, a.voxel[1], a.origin[1]);
     const float pz = __fmaf_rn((float)iz, a.voxel[2], a.origin[2]);
+    if (ARITH == kStrict) {
+        // the products c_v.y * py of the STRICT numerator, two layers per lane, rounded as the
+        // reference rounds them; walk_exact loads them, so no packed product feeds its sums
+        // (the code generator contracts a packed multiply into the packed add that consumes it)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int k = 2 * c + h;
+            if (k < ey)
+                s_meta[g].T[k] = __fmul_rn(cv1, __fadd_rn(__fmul_rn(__uint2float_rn((uint32_t)(a.vmin[1] + by0 + k)),
+                                                                     a.voxel[1]), a.origin[1]));
+        }
+    }
     const float nu = __fmaf_rn(cu0, px, __fmaf_rn(cu1, py, __fmaf_rn(cu2, pz, cu3)));
     const float nv = __fmaf_rn(cv0, px, __fmaf_rn(cv1, py, __fmaf_rn(cv2, pz, cv3)));
     const float nw = __fmaf_rn(cw0, px, __fmaf_rn(cw1, py, __fmaf_rn(cw2, pz, cw3)));
@@ -541,27 +554,15 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
     return 1;
 }
 
-// y positions {py[2m], py[2m + 1]} of a column as a register pair
-template <int N>
-__device__ __forceinline__ uint64_t ypair(const float (&py)[N], int m)
-{
-    return f2pack(py[2 * m], py[2 * m + 1]);
-}
-template <int N>
-__device__ __forceinline__ uint64_t ypair(const uint64_t (&py2)[N], int m)
-{
-    return py2[m];
-}
-
 // STRICT-contract walk of an untilted column (same calls and return value as walk_fast),
 // bit-identical to the reference's per-voxel division: n_v = ((c.x*px + c.y*py) + c.z*pz)
-// + c.w in the reference's order, v = n_v / n_w by div_exact with the column's n_w, and
-// the pixel by pix_bits2.  Returns -1, without calling f, when the projection's operands
+// + c.w in the reference's order (c.y*py = Tk[k], formed by compute_meta), v = n_v / n_w by
+// div_exact with the column's n_w, and the pixel by pix_bits2.  Returns -1, without calling f, when the projection's operands
 // failed div_exact's screen over the brick (compute_meta; the caller then divides per
 // voxel).
-template <int LEN, typename PY, typename F>
+template <int LEN, typename F>
 __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a, float nu, float nw, float Pv,
-                                          float Rv, const PY &py2, F &&f)
+                                          float Rv, const float *__restrict__ Tk, F &&f)
 {
     static_assert(LEN % 2 == 0, "columns are walked two voxels at a time");
     const float4 cv = M.cv;
@@ -573,12 +574,12 @@ __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a
     const float ylo = __fmul_rn(__fmaf_rn(-nw, y, 1.0f), y);
     const float qu = div_exact(nu, -nw, y, ylo);
     const uint32_t du = pix_bits(qu) - (kMagic + (uint32_t)rc.x);
-    const uint64_t cvy = f2pack(cv.y, cv.y), P2 = f2pack(Pv, Pv), R2 = f2pack(Rv, Rv), W2 = f2pack(cv.w, cv.w);
+    const uint64_t P2 = f2pack(Pv, Pv), R2 = f2pack(Rv, Rv), W2 = f2pack(cv.w, cv.w);
     const uint64_t Y2 = f2pack(y, y), YL2 = f2pack(ylo, ylo), NB2 = f2pack(-nw, -nw);
     const uint64_t half = f2pack(0.5f, 0.5f), magic = f2pack(8388608.0f, 8388608.0f);
     const uint32_t base_v = kMagic + (uint32_t)a.row_off_f + (uint32_t)rc.z;
-    auto qv = [&](int m) {
-        const uint64_t nv = add2(add2(add2(P2, mul2(ypair(py2, m), cvy)), R2), W2);
+    auto qv = [&](int m) {  // Tk: shared memory, {T[2m], T[2m + 1]} as one 64-bit load
+        const uint64_t nv = add2(add2(add2(P2, reinterpret_cast<const uint64_t *>(Tk)[m]), R2), W2);
         return div_exact2(nv, NB2, Y2, YL2);
     };
     if (M.flags.w) {
@@ -621,7 +622,7 @@ __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a
 // warp meets the projection's u range; 2 when the inside path ran; 1 otherwise.
 template <int ARITH, int LEN, typename PY, typename F>
 __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &a, int ax, int az, const PY &py2,
-                                           F &&f)
+                                           const float *__restrict__ Tk, F &&f)
 {
     const float4 cu = M.cu, cv = M.cv, cw = M.cw;
     const uint4 tgt = M.tgt;
@@ -639,7 +640,7 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
             // column invariants
             const float nu = num_strict(cu, px, 0.0f, pz);
             const float nw = num_strict(cw, px, 0.0f, pz);
-            const int w = walk_exact<LEN>(M, a, nu, nw, __fmul_rn(cv.x, px), __fmul_rn(cv.z, pz), py2, f);
+            const int w = walk_exact<LEN>(M, a, nu, nw, __fmul_rn(cv.x, px), __fmul_rn(cv.z, pz), Tk, f);
             if (w >= 0) return w;
             const uint32_t du = (uint32_t)(__float2int_rz(roundf(__fdiv_rn(nu, nw))) - rc.x);
             const bool in_u = du < (uint32_t)rc.y;
@@ -716,7 +717,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
     const int e_end = min((int)a.n_entries, e_begin + (int)a.per_split);
 
     for (int e0 = e_begin; e0 < e_end; e0 += G) {
-        if (warp == 0) compute_meta<LIST, false>(s_meta, pd, a, e0, e_end, x0, y0, z0, BX, BY, BZ, lane);
+        if (warp == 0) compute_meta<ARITH, LIST, false>(s_meta, pd, a, e0, e_end, x0, y0, z0, BX, BY, BZ, lane);
         __syncthreads();
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
@@ -775,7 +776,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 auto splat = [&](const uint4 *vals, float nu, float nw, float Pv, float Rv) {
                     uint4 quad;
                     // a zero adds nothing to a shared-memory tile; no test for it
-                    walk_exact<BY>(M, a, nu, nw, Pv, Rv, py, [&](auto, int k, bool in, uint32_t idx) {
+                    walk_exact<BY>(M, a, nu, nw, Pv, Rv, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
                         if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
                         const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
                         if (in) atomicAdd(&tile[idx], v);
@@ -816,13 +817,13 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 const int ax = a.vmin[0] + x0 + cx, az = a.vmin[2] + z0 + cz;
                 if (ARITH != kFast && fl.x == kTile) {
                     // a zero adds nothing to a shared-memory tile; no test for it
-                    walk_column<ARITH, BY>(M, a, ax, az, py, [&](auto, int k, bool in, uint32_t idx) {
+                    walk_column<ARITH, BY>(M, a, ax, az, py, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
                         if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
                         const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
                         if (in) atomicAdd(&tile[idx], v);
                     });
                 } else {
-                    walk_column<ARITH, BY>(M, a, ax, az, py, [&](auto, int k, bool in, uint32_t idx) {
+                    walk_column<ARITH, BY>(M, a, ax, az, py, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
                         if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
                         const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
                         if (in & (v != 0u)) atomicAdd(&sum[idx], v);
@@ -993,11 +994,11 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
     // metadata double buffer (s_meta holds 2 * G entries): warp 0 prepares the next group
     // while the CTA walks the current one, so one barrier per group suffices
     const int n_entries = (int)a.n_entries;
-    if (warp == 0) compute_meta<LIST, true>(s_meta, pd, a, 0, n_entries, x0, y0, z0, BX, CB, BWD_BZ, lane);
+    if (warp == 0) compute_meta<ARITH, LIST, true>(s_meta, pd, a, 0, n_entries, x0, y0, z0, BX, CB, BWD_BZ, lane);
     __syncthreads();
     for (int e0 = 0, buf = 0; e0 < n_entries; e0 += G, buf ^= G) {
         if (warp == 0 && e0 + G < n_entries)
-            compute_meta<LIST, true>(s_meta + (buf ^ G), pd, a, e0 + G, n_entries, x0, y0, z0, BX, CB, BWD_BZ,
+            compute_meta<ARITH, LIST, true>(s_meta + (buf ^ G), pd, a, e0 + G, n_entries, x0, y0, z0, BX, CB, BWD_BZ,
                                      lane);
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
@@ -1024,7 +1025,7 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
                     }
                 }
             };
-            const int walked = walk_column<ARITH, CB>(M, a, ax, az, py, [&](auto inside, int k, bool in, uint32_t idx) {
+            const int walked = walk_column<ARITH, CB>(M, a, ax, az, py, M.T, [&](auto inside, int k, bool in, uint32_t idx) {
                 rb[k] = 0u;
                 if (in) rb[k] = load_ratio_bits<DT>(ratio, idx);
                 if constexpr (!decltype(inside)::value) {
