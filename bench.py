@@ -85,9 +85,26 @@ CONFIGS = {
 FLOPS_PER_PAIR = 44          # algorithmic FP32 operations per (voxel, projection) pair, forward + backward
 NOMINAL_FP32_LANES = 148 * 128
 # DRAM bytes (read + write) per voxel per launch, from one ncu capture of each kernel on the
-# c2 geometry's central 256-layer slab (FAST contract, FP32 storage: 718.1 MB and 1210.0 MB
-# for 150,994,944 voxels); scaled to a launch by its voxel count for the same geometry
-MEASURED_TRAFFIC_PER_VOXEL = {"forward": 716.1e6 / 150994944, "backward": 1219.0e6 / 150994944}
+# c2 geometry's central 256-layer slab (150,994,944 voxels, FP32 storage); scaled to a
+# launch by its voxel count for the same geometry
+MEASURED_TRAFFIC_PER_VOXEL = {
+    "strict": {"forward": 716.1e6 / 150994944, "backward": 1212.8e6 / 150994944},
+    "fast": {"forward": 716.1e6 / 150994944, "backward": 1219.0e6 / 150994944},
+}
+# executed-work figures of the same captures (profiles/k_*_c2slab.md): issue-active share,
+# l1tex (shared-memory pipe) throughput and thread instructions per (voxel, projection) pair
+MEASURED_PROFILE = {
+    "strict": {"forward": {"issue_active_pct": 79.6, "l1tex_pct": 71.3, "fma_pipe_pct": 48.8,
+                           "thread_inst_per_pair": 20.7},
+               "backward": {"issue_active_pct": 66.2, "l1tex_pct": 49.7, "fma_pipe_pct": 62.9,
+                            "thread_inst_per_pair": 15.5},
+               "source": "ncu --set full, c2 geometry 256-layer slab: profiles/k_forward_tiled_strict_c2slab.md, "
+                         "profiles/k_backward_tiled_strict_c2slab.md"},
+    "fast": {"forward": {"issue_active_pct": 76.0, "l1tex_pct": 84.9, "thread_inst_per_pair": 13.0},
+             "backward": {"issue_active_pct": 68.7, "thread_inst_per_pair": 11.5},
+             "source": "ncu --set full, c2 geometry 256-layer slab: profiles/k_forward_tiled_fast_c2slab.md, "
+                       "profiles/k_backward_tiled_fast_c2slab.md"},
+}
 
 
 def parse_args():
@@ -597,7 +614,7 @@ def run_ours(args, cfg, rank, world, local):
     achieved = alg_bytes / (dom_ms / 1000.0) / 1e9
     traffic = None
     if args.config in ("c2", "c2slab") and args.storage == "fp32":
-        traffic = MEASURED_TRAFFIC_PER_VOXEL[dom] * prob.nvox
+        traffic = MEASURED_TRAFFIC_PER_VOXEL[args.arith][dom] * prob.nvox
     sm_mhz = (clk or {}).get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = NOMINAL_FP32_LANES * 2 * float(sm_mhz) * 1e6 / 1e12
     step_ms = total_ms / K
@@ -627,7 +644,10 @@ def run_ours(args, cfg, rank, world, local):
                              "traffic scaled from an ncu capture of the 256-layer slab by voxel count"},
         "compute": {"flops_per_pair": FLOPS_PER_PAIR, "achieved_tflops": FLOPS_PER_PAIR * pairs_step / (step_ms / 1000) / 1e12,
                     "peak_fp32_tflops": fp32_peak, "frac": FLOPS_PER_PAIR * pairs_step / (step_ms / 1000) / 1e12 / fp32_peak,
-                    "peak_source": "nominal: 148 SM x 128 FP32 lanes x 2 x median SM clock"},
+                    "peak_source": "nominal: 148 SM x 128 FP32 lanes x 2 x median SM clock",
+                    "note": "44 algorithmic flop per pair (the reference's operations), not the executed "
+                            "instructions: see profile"},
+        "profile": MEASURED_PROFILE[args.arith],
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
