@@ -868,9 +868,11 @@ def run_serving(args, cfg, rank, world, local):
                   "geometry": {"so": 100.0, "sd": 1000.0, "angle": 360.0}, "detector": {"px": cfg["px"]}}
         reqs.append((params, (e, P)))
     arrivals = np.cumsum(rng.exponential(1.0 / cfg["rate"], n))
-    # page-locked result buffers (a serving client's own); requests of one kind share one,
-    # as the benchmark reads no result
-    out_of = {k: torch.empty(data[k][1], dtype=torch.float32, pin_memory=True).numpy() for k in kinds}
+    # page-locked result buffers (a serving client's own); requests of one volume size share
+    # one, as the benchmark reads no result
+    out_by_edge = {e: torch.empty(max(data[k][1] for k in kinds if k[0] == e), dtype=torch.float32,
+                                  pin_memory=True).numpy() for e in cfg["edges"]}
+    out_of = {k: out_by_edge[k[0]][:data[k][1]] for k in kinds}
     outs = [out_of[k] for _, k in reqs]
     pairs_of = {k: data[k][1] * k[1] for k in kinds}  # N x P per reconstruction (it 1)
     total_pairs = sum(pairs_of[k] for _, k in reqs) * cfg["it"]

@@ -77,7 +77,7 @@ struct __align__(16) ProjMeta {
 // per-projection metadata: one group of G entries, computed by warp 0
 // lane = g * 8 + corner of the brick [x0, x0+ex) x [y0, y0+ey) x [z0, z0+ez)
 // --------------------------------------------------------------------------------------
-template <int ARITH, bool LIST, bool GATHER>
+template <int ARITH, bool LIST, bool GATHER, int TCAP = TILE_CAP>
 __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdata *__restrict__ pd,
                                              const LaunchArgs &a, int e0, int e_end, int bx0, int by0, int bz0,
                                              int ex, int ey, int ez, int lane)
@@ -161,7 +161,7 @@ __device__ __forceinline__ void compute_meta(ProjMeta *s_meta, const xpr_projdat
             t = min(t, ft);
         }
         const int area = (r - l) * (t - b);
-        const int mode = (!valid || r <= l || t <= b) ? kSkip : ((ok && area <= TILE_CAP) ? kTile : kDirect);
+        const int mode = (!valid || r <= l || t <= b) ? kSkip : ((ok && area <= TCAP) ? kTile : kDirect);
         const uint32_t img_base = img * a.img_stride;
         const bool tile = (mode == kTile) && !GATHER;
         const uint32_t pitch = tile ? (uint32_t)(r - l) : a.det_w;
@@ -560,11 +560,13 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
 // div_exact with the column's n_w, and the pixel by pix_bits2.  Returns -1, without calling f, when the projection's operands
 // failed div_exact's screen over the brick (compute_meta; the caller then divides per
 // voxel).
-template <int LEN, typename F>
+// CHUNK < LEN walks the column as LEN / CHUNK unrolled chunks in a rolled loop (fewer
+// values live at once); f then sees k whose low bits are compile-time constants.
+template <int LEN, int CHUNK = LEN, typename F>
 __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a, float nu, float nw, float Pv,
                                           float Rv, const float *__restrict__ Tk, F &&f)
 {
-    static_assert(LEN % 2 == 0, "columns are walked two voxels at a time");
+    static_assert(LEN % 2 == 0 && CHUNK % 4 == 0 && LEN % CHUNK == 0, "columns are walked two voxels at a time");
     const float4 cv = M.cv;
     const int4 rc = M.rect;
     const uint4 tgt = M.tgt;
@@ -585,12 +587,16 @@ __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a
     if (M.flags.w) {
         // inside: every pixel is in the rectangle, idx = bits * pitch + K (mod 2^32)
         const uint32_t K = du + tgt.y - base_v * pitch;
+#pragma unroll 1
+        for (int c0 = 0; c0 < LEN; c0 += CHUNK) {
 #pragma unroll
-        for (int k = 0; k < LEN; k += 2) {
-            uint32_t b0, b1;
-            u2unpack(pix_bits2(qv(k >> 1), half, magic), b0, b1);
-            f(std::true_type{}, k, true, b0 * pitch + K);
-            f(std::true_type{}, k + 1, true, b1 * pitch + K);
+            for (int kk = 0; kk < CHUNK; kk += 2) {
+                const int k = c0 + kk;
+                uint32_t b0, b1;
+                u2unpack(pix_bits2(qv(k >> 1), half, magic), b0, b1);
+                f(std::true_type{}, k, true, b0 * pitch + K);
+                f(std::true_type{}, k + 1, true, b1 * pitch + K);
+            }
         }
         return 2;
     }
@@ -598,16 +604,20 @@ __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a
     if (!__any_sync(0xffffffffu, in_u)) return 0;
     const uint32_t K = du + tgt.y;
     const float ex = __fsub_rn(a.row_off_f, 0.5f);  // pix_bits2's one exception
+#pragma unroll 1
+    for (int c0 = 0; c0 < LEN; c0 += CHUNK) {
 #pragma unroll
-    for (int k = 0; k < LEN; k += 2) {
-        const uint64_t q = qv(k >> 1);
-        uint32_t b0, b1;
-        float q0, q1;
-        u2unpack(pix_bits2(q, half, magic), b0, b1);
-        f2unpack(q, q0, q1);
-        const uint32_t dv0 = b0 - base_v, dv1 = b1 - base_v;
-        f(std::false_type{}, k, in_u && (dv0 < (uint32_t)rc.w) && (q0 != ex), dv0 * pitch + K);
-        f(std::false_type{}, k + 1, in_u && (dv1 < (uint32_t)rc.w) && (q1 != ex), dv1 * pitch + K);
+        for (int kk = 0; kk < CHUNK; kk += 2) {
+            const int k = c0 + kk;
+            const uint64_t q = qv(k >> 1);
+            uint32_t b0, b1;
+            float q0, q1;
+            u2unpack(pix_bits2(q, half, magic), b0, b1);
+            f2unpack(q, q0, q1);
+            const uint32_t dv0 = b0 - base_v, dv1 = b1 - base_v;
+            f(std::false_type{}, k, in_u && (dv0 < (uint32_t)rc.w) && (q0 != ex), dv0 * pitch + K);
+            f(std::false_type{}, k + 1, in_u && (dv1 < (uint32_t)rc.w) && (q1 != ex), dv1 * pitch + K);
+        }
     }
     return 1;
 }
@@ -620,7 +630,9 @@ __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a
 // viewport (flags.w) skips the bounds tests: `inside` is then std::true_type and
 // `in` is true for every voxel.  Returns 0, without calling f, when no column of the
 // warp meets the projection's u range; 2 when the inside path ran; 1 otherwise.
-template <int ARITH, int LEN, typename PY, typename F>
+// CHUNK < LEN: the STRICT walks run as LEN / CHUNK unrolled chunks in a rolled loop (as in
+// walk_exact); py2 must then be indexable at run time (the shared-memory pairs).
+template <int ARITH, int LEN, int CHUNK = LEN, typename PY, typename F>
 __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &a, int ax, int az, const PY &py2,
                                            const float *__restrict__ Tk, F &&f)
 {
@@ -640,22 +652,29 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
             // column invariants
             const float nu = num_strict(cu, px, 0.0f, pz);
             const float nw = num_strict(cw, px, 0.0f, pz);
-            const int w = walk_exact<LEN>(M, a, nu, nw, __fmul_rn(cv.x, px), __fmul_rn(cv.z, pz), Tk, f);
+            const int w = walk_exact<LEN, CHUNK>(M, a, nu, nw, __fmul_rn(cv.x, px), __fmul_rn(cv.z, pz), Tk, f);
             if (w >= 0) return w;
             const uint32_t du = (uint32_t)(__float2int_rz(roundf(__fdiv_rn(nu, nw))) - rc.x);
             const bool in_u = du < (uint32_t)rc.y;
             if (!__any_sync(0xffffffffu, in_u)) return 0;
             const uint32_t K = du + tgt.y;
             const float Pv = __fmul_rn(cv.x, px), Rv = __fmul_rn(cv.z, pz);
+#pragma unroll 1
+            for (int c0 = 0; c0 < LEN; c0 += CHUNK) {
 #pragma unroll
-            for (int k = 0; k < LEN; ++k) {
-                const float nv = __fadd_rn(__fadd_rn(__fadd_rn(Pv, __fmul_rn(cv.y, ypos(py2, k))), Rv), cv.w);
-                const uint32_t dv = (uint32_t)(__float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off))) - rc.z);
-                f(std::false_type{}, k, in_u && (dv < (uint32_t)rc.w), dv * pitch + K);
+                for (int kk = 0; kk < CHUNK; ++kk) {
+                    const int k = c0 + kk;
+                    const float nv = __fadd_rn(__fadd_rn(__fadd_rn(Pv, __fmul_rn(cv.y, ypos(py2, k))), Rv), cv.w);
+                    const uint32_t dv = (uint32_t)(__float2int_rz(roundf(__fsub_rn(__fdiv_rn(nv, nw), off))) - rc.z);
+                    f(std::false_type{}, k, in_u && (dv < (uint32_t)rc.w), dv * pitch + K);
+                }
             }
         } else {
+#pragma unroll 1
+            for (int c0 = 0; c0 < LEN; c0 += CHUNK)
 #pragma unroll
-            for (int k = 0; k < LEN; ++k) {
+            for (int kk = 0; kk < CHUNK; ++kk) {
+                const int k = c0 + kk;
                 const float py = ypos(py2, k);
                 const float nu = num_strict(cu, px, py, pz);
                 const float nv = num_strict(cv, px, py, pz);
@@ -672,21 +691,35 @@ __device__ __forceinline__ int walk_column(const ProjMeta &M, const LaunchArgs &
 // --------------------------------------------------------------------------------------
 // forward
 // --------------------------------------------------------------------------------------
-constexpr size_t kFwdSmem = (size_t)(BY / 4 * BZ * VSTRIDE + G * TILE_CAP) * sizeof(uint32_t);
+// Forward brick shapes: 32 x by x 32 voxels, nt threads (cols = 1024 / nt columns of by
+// layers per thread), G shared-memory tiles of `tile` pixels.  The narrow shape serves the
+// FAST contract and the batched kernels; the STRICT contract's per-column work (reciprocal,
+// u pixel, the packing of the column's constants) is a larger share of a voxel's, so its
+// single-problem forward walks 16-layer columns (the tall shape) to halve that share.
+template <int BY_, int NT_, int TC_>
+struct FwdShape {
+    static constexpr int by = BY_, nt = NT_, tile = TC_, warps = NT_ / 32, cols = BX * BZ / NT_;
+    static constexpr size_t smem = (size_t)(BY_ / 4 * BZ * VSTRIDE + G * TC_) * sizeof(uint32_t);
+    static_assert(BY_ % 4 == 0 && BY_ <= 16 && BX * BZ % NT_ == 0, "forward brick shape");
+};
+using FwdNarrow = FwdShape<BY, NT, TILE_CAP>;
+using FwdTall = FwdShape<16, 512, 2048>;
+constexpr size_t kFwdSmem = FwdNarrow::smem;
 
 // One forward work unit: brick `brick` (x fastest, then z, then y) against the
 // projection run `split` (entries [split * per_split, (split + 1) * per_split)).
 // Called by every thread of the CTA; returns with the CTA converged.
-template <int ARITH, bool LIST>
+template <int ARITH, bool LIST, typename SH = FwdNarrow>
 __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint32_t *__restrict__ sum,
                                              const xpr_projdata *__restrict__ pd, const LaunchArgs &a,
                                              uint32_t brick, uint32_t split, int bricks_x, int bricks_z,
                                              uint32_t *smem, ProjMeta *s_meta)
 {
-    // fixed-point values [BY / 4][BZ][VSTRIDE]: layers 4m .. 4m + 3 of (x, z) are adjacent
+    constexpr int BYF = SH::by, NTF = SH::nt, TCF = SH::tile, NW = SH::warps, CPT = SH::cols;
+    // fixed-point values [BYF / 4][BZ][VSTRIDE]: layers 4m .. 4m + 3 of (x, z) are adjacent
     // words, so a thread reads four of its column's voxels with one 128-bit load
     uint32_t *s_val = smem;
-    uint32_t *s_tile = smem + BY / 4 * BZ * VSTRIDE;   // [G][TILE_CAP]
+    uint32_t *s_tile = smem + BYF / 4 * BZ * VSTRIDE;   // [G][TCF]
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int b = (int)brick;
@@ -694,11 +727,11 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
     b /= bricks_x;
     const int bzi = b % bricks_z;
     const int byi = b / bricks_z;
-    const int x0 = bxi * BX, y0 = byi * BY, z0 = bzi * BZ;
+    const int x0 = bxi * BX, y0 = byi * BYF, z0 = bzi * BZ;
     const int sx = a.size[0], sy = a.size[1], sz = a.size[2];
 
     bool any = false;
-    for (int i = threadIdx.x; i < BX * BY * BZ; i += NT) {
+    for (int i = threadIdx.x; i < BX * BYF * BZ; i += NTF) {
         const int x = i & 31, z = (i >> 5) & 31, y = i >> 10;
         const int gx = x0 + x, gy = y0 + y, gz = z0 + z;
         uint32_t v = 0;
@@ -706,18 +739,32 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
         s_val[((y >> 2) * BZ + z) * VSTRIDE + 4 * x + (y & 3)] = v;
         any |= (v != 0u);
     }
-    for (int i = threadIdx.x; i < G * TILE_CAP; i += NT) s_tile[i] = 0u;
-    if (!__syncthreads_or(any)) return;   // an all-zero brick adds nothing
-
-    float py[BY];
+    for (int i = threadIdx.x; i < G * TCF; i += NTF) s_tile[i] = 0u;
+    // the column's y positions: registers for 8-layer columns; for 16-layer columns (STRICT,
+    // whose exact walk reads only the c_v.y*py products) in shared memory as pairs, for the
+    // per-voxel fallback
+    constexpr bool PYREG = BYF <= 8;
+    float py[PYREG ? BYF : 2];
+    __shared__ __align__(16) uint64_t s_py2[8];
+    if (PYREG) {
 #pragma unroll
-    for (int k = 0; k < BY; ++k) py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
+        for (int k = 0; k < BYF; ++k) py[k] = pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]);
+    } else if (threadIdx.x < BYF / 2) {
+        const int k = 2 * (int)threadIdx.x;
+        s_py2[threadIdx.x] = f2pack(pos<ARITH>(a.vmin[1] + y0 + k, a.voxel[1], a.origin[1]),
+                                    pos<ARITH>(a.vmin[1] + y0 + k + 1, a.voxel[1], a.origin[1]));
+    }
+    auto with_py = [&](auto &&fn) {
+        if constexpr (PYREG) fn(py);
+        else fn(s_py2);
+    };
+    if (!__syncthreads_or(any)) return;   // an all-zero brick adds nothing
 
     const int e_begin = (int)split * (int)a.per_split;
     const int e_end = min((int)a.n_entries, e_begin + (int)a.per_split);
 
     for (int e0 = e_begin; e0 < e_end; e0 += G) {
-        if (warp == 0) compute_meta<ARITH, LIST, false>(s_meta, pd, a, e0, e_end, x0, y0, z0, BX, BY, BZ, lane);
+        if (warp == 0) compute_meta<ARITH, LIST, false, TCF>(s_meta, pd, a, e0, e_end, x0, y0, z0, BX, BYF, BZ, lane);
         __syncthreads();
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
@@ -726,9 +773,9 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
             const ProjMeta M = s_meta[g];
             const int4 fl = M.flags;
             if (fl.x == kSkip) continue;
-            uint32_t *tile = s_tile + g * TILE_CAP;
+            uint32_t *tile = s_tile + g * TCF;
             const bool orx = fl.y;
-            if (ARITH == kFast && fl.x == kTile) {
+            if constexpr (ARITH == kFast) if (fl.x == kTile) {
                 // FAST into a tile: one lane coordinate is the thread's for all of its columns,
                 // so its share of the column numerators C = fma(c.x, px, c.w) + c.z * pz is
                 // computed once per projection
@@ -736,7 +783,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 auto splat = [&](const uint4 *vals, float Cu, float Cv, float Cw) {
                     uint4 quad;
                     // a zero adds nothing to a shared-memory tile; no test for it
-                    walk_fast<BY>(M, a, Cu, Cv, Cw, py, [&](auto, int k, bool in, uint32_t idx) {
+                    walk_fast<BYF>(M, a, Cu, Cv, Cw, py, [&](auto, int k, bool in, uint32_t idx) {
                         if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
                         const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
                         if (in) atomicAdd(&tile[idx], v);
@@ -746,8 +793,8 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                     const float pz = pos<kFast>(a.vmin[2] + z0 + lane, a.voxel[2], a.origin[2]);
                     const float Pu = __fmul_rn(cu.z, pz), Pv = __fmul_rn(cv.z, pz), Pw = __fmul_rn(cw.z, pz);
 #pragma unroll 1
-                    for (int j = 0; j < 4; ++j) {
-                        const int cx = warp + 8 * j;
+                    for (int j = 0; j < CPT; ++j) {
+                        const int cx = warp + NW * j;
                         const float px = pos<kFast>(a.vmin[0] + x0 + cx, a.voxel[0], a.origin[0]);
                         splat(reinterpret_cast<const uint4 *>(s_val + lane * VSTRIDE + 4 * cx),
                               __fadd_rn(__fmaf_rn(cu.x, px, cu.w), Pu), __fadd_rn(__fmaf_rn(cv.x, px, cv.w), Pv),
@@ -758,8 +805,8 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                     const float Au = __fmaf_rn(cu.x, px, cu.w), Av = __fmaf_rn(cv.x, px, cv.w),
                                 Aw = __fmaf_rn(cw.x, px, cw.w);
 #pragma unroll 1
-                    for (int j = 0; j < 4; ++j) {
-                        const int cz = warp + 8 * j;
+                    for (int j = 0; j < CPT; ++j) {
+                        const int cz = warp + NW * j;
                         const float pz = pos<kFast>(a.vmin[2] + z0 + cz, a.voxel[2], a.origin[2]);
                         splat(reinterpret_cast<const uint4 *>(s_val + cz * VSTRIDE + 4 * lane),
                               __fadd_rn(Au, __fmul_rn(cu.z, pz)), __fadd_rn(Av, __fmul_rn(cv.z, pz)),
@@ -768,7 +815,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 }
                 continue;
             }
-            if (ARITH == kStrict && fl.x == kTile && (fl.z & 2)) {
+            if constexpr (ARITH == kStrict) if (fl.x == kTile && (fl.z & 2)) {
                 // STRICT into a tile, untilted and screened: n_u and n_w are (c.x*px + c.z*pz) + c.w
                 // (c.y*py is a zero), so the lane coordinate's product in every row is formed once
                 // per projection; walk_exact divides per voxel with the column's reciprocal
@@ -776,7 +823,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 auto splat = [&](const uint4 *vals, float nu, float nw, float Pv, float Rv) {
                     uint4 quad;
                     // a zero adds nothing to a shared-memory tile; no test for it
-                    walk_exact<BY>(M, a, nu, nw, Pv, Rv, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
+                    walk_exact<BYF, 8>(M, a, nu, nw, Pv, Rv, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
                         if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
                         const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
                         if (in) atomicAdd(&tile[idx], v);
@@ -786,8 +833,8 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                     const float pz = pos<kStrict>(a.vmin[2] + z0 + lane, a.voxel[2], a.origin[2]);
                     const float Bu = __fmul_rn(cu.z, pz), Bw = __fmul_rn(cw.z, pz), Rv = __fmul_rn(cv.z, pz);
 #pragma unroll 1
-                    for (int j = 0; j < 4; ++j) {
-                        const int cx = warp + 8 * j;
+                    for (int j = 0; j < CPT; ++j) {
+                        const int cx = warp + NW * j;
                         const float px = pos<kStrict>(a.vmin[0] + x0 + cx, a.voxel[0], a.origin[0]);
                         splat(reinterpret_cast<const uint4 *>(s_val + lane * VSTRIDE + 4 * cx),
                               __fadd_rn(__fadd_rn(__fmul_rn(cu.x, px), Bu), cu.w),
@@ -797,8 +844,8 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                     const float px = pos<kStrict>(a.vmin[0] + x0 + lane, a.voxel[0], a.origin[0]);
                     const float Au = __fmul_rn(cu.x, px), Aw = __fmul_rn(cw.x, px), Pv = __fmul_rn(cv.x, px);
 #pragma unroll 1
-                    for (int j = 0; j < 4; ++j) {
-                        const int cz = warp + 8 * j;
+                    for (int j = 0; j < CPT; ++j) {
+                        const int cz = warp + NW * j;
                         const float pz = pos<kStrict>(a.vmin[2] + z0 + cz, a.voxel[2], a.origin[2]);
                         splat(reinterpret_cast<const uint4 *>(s_val + cz * VSTRIDE + 4 * lane),
                               __fadd_rn(__fadd_rn(Au, __fmul_rn(cu.z, pz)), cu.w),
@@ -807,26 +854,30 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 }
                 continue;
             }
-            // 4 columns per thread; lanes run across the ray so a warp hits distinct pixels
+            // CPT columns per thread; lanes run across the ray so a warp hits distinct pixels
 #pragma unroll 1
-            for (int j = 0; j < 4; ++j) {
-                const int cx = orx ? warp + 8 * j : lane;
-                const int cz = orx ? lane : warp + 8 * j;
+            for (int j = 0; j < CPT; ++j) {
+                const int cx = orx ? warp + NW * j : lane;
+                const int cz = orx ? lane : warp + NW * j;
                 const uint4 *vals = reinterpret_cast<const uint4 *>(s_val + cz * VSTRIDE + 4 * cx);
                 uint4 quad;
                 const int ax = a.vmin[0] + x0 + cx, az = a.vmin[2] + z0 + cz;
                 if (ARITH != kFast && fl.x == kTile) {
                     // a zero adds nothing to a shared-memory tile; no test for it
-                    walk_column<ARITH, BY>(M, a, ax, az, py, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
-                        if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
-                        const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
-                        if (in) atomicAdd(&tile[idx], v);
+                    with_py([&](const auto &pyv) {
+                        walk_column<ARITH, BYF, (BYF > 8 ? 8 : BYF)>(M, a, ax, az, pyv, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
+                            if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
+                            const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
+                            if (in) atomicAdd(&tile[idx], v);
+                        });
                     });
                 } else {
-                    walk_column<ARITH, BY>(M, a, ax, az, py, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
-                        if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
-                        const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
-                        if (in & (v != 0u)) atomicAdd(&sum[idx], v);
+                    with_py([&](const auto &pyv) {
+                        walk_column<ARITH, BYF, (BYF > 8 ? 8 : BYF)>(M, a, ax, az, pyv, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
+                            if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
+                            const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
+                            if (in & (v != 0u)) atomicAdd(&sum[idx], v);
+                        });
                     });
                 }
             }
@@ -837,10 +888,10 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
         for (int g = 0; g < G; ++g) {
             const ProjMeta &M = s_meta[g];
             if (M.flags.x != kTile) continue;
-            uint32_t *tile = s_tile + g * TILE_CAP;
+            uint32_t *tile = s_tile + g * TCF;
             const int4 rc = M.rect;
             const int tw = rc.y, th = rc.w;
-            for (int r = warp; r < th; r += NT / 32) {
+            for (int r = warp; r < th; r += NW) {
                 uint32_t *dst = sum + M.tgt.z + (uint32_t)(rc.z + r) * a.det_w + (uint32_t)rc.x;
                 for (int c = lane; c < tw; c += 32) {
                     const uint32_t v = tile[r * tw + c];
@@ -855,15 +906,19 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
     }
 }
 
-template <int ARITH, bool LIST>
-__global__ void __launch_bounds__(NT, 4)
+template <int ARITH, bool LIST, typename SH>
+__global__ void __launch_bounds__(SH::nt, 1024 / SH::nt)
     k_forward_tiled(const float *__restrict__ vol, uint32_t *__restrict__ sum, const xpr_projdata *__restrict__ pd,
                     const LaunchArgs a, int bricks_x, int bricks_z)
 {
     extern __shared__ uint32_t smem[];
     __shared__ ProjMeta s_meta[G];
-    forward_unit<ARITH, LIST>(vol, sum, pd, a, blockIdx.x, blockIdx.y, bricks_x, bricks_z, smem, s_meta);
+    forward_unit<ARITH, LIST, SH>(vol, sum, pd, a, blockIdx.x, blockIdx.y, bricks_x, bricks_z, smem, s_meta);
 }
+
+// the forward shape of each contract's single-problem kernel
+template <int ARITH>
+using FwdShapeOf = typename std::conditional<ARITH == kStrict, FwdTall, FwdNarrow>::type;
 
 // Work-items of the reference NDRange padding (kernel.hpp:73-81, H5): one thread each,
 // voxel coordinates from to3D() (utils.cl:39-45), all projections, global atomics.
@@ -1370,11 +1425,14 @@ cudaError_t prepare_device_kernels()
     if (e != cudaSuccess) return e;
     if (dev < 64 && g_attr_done[dev]) return cudaSuccess;
     const int smem = (int)kFwdSmem;
-    void (*fns[])(const float *, uint32_t *, const xpr_projdata *, const LaunchArgs, int, int) = {
-        k_forward_tiled<kStrict, false>, k_forward_tiled<kStrict, true>, k_forward_tiled<kFast, false>,
-        k_forward_tiled<kFast, true>};
-    for (auto f : fns) {
-        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    using FwdFn = void (*)(const float *, uint32_t *, const xpr_projdata *, const LaunchArgs, int, int);
+    const struct { FwdFn f; size_t smem; } fns[] = {
+        {k_forward_tiled<kStrict, false, FwdShapeOf<kStrict>>, FwdShapeOf<kStrict>::smem},
+        {k_forward_tiled<kStrict, true, FwdShapeOf<kStrict>>, FwdShapeOf<kStrict>::smem},
+        {k_forward_tiled<kFast, false, FwdShapeOf<kFast>>, FwdShapeOf<kFast>::smem},
+        {k_forward_tiled<kFast, true, FwdShapeOf<kFast>>, FwdShapeOf<kFast>::smem}};
+    for (const auto &f : fns) {
+        e = cudaFuncSetAttribute(f.f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem);
         if (e != cudaSuccess) return e;
     }
     void (*bfns[])(const BatchFwdItem *, int, uint32_t, uint32_t *) = {k_forward_batched<kStrict>,
@@ -1387,16 +1445,16 @@ cudaError_t prepare_device_kernels()
     return cudaSuccess;
 }
 
-cudaError_t launch_forward(const float *vol, uint32_t *sum, const xpr_projdata *pd, const LaunchArgs &a0, int arith,
-                           int compat_pad, const DeviceInfo &dev, cudaStream_t s)
+// the single-problem forward of contract AR over its brick shape
+template <int AR>
+static cudaError_t forward_tiled(const float *vol, uint32_t *sum, const xpr_projdata *pd, LaunchArgs a,
+                                 const DeviceInfo &dev, cudaStream_t s)
 {
-    cudaError_t e = prepare_device_kernels();
-    if (e != cudaSuccess) return e;
-    LaunchArgs a = a0;
-    const int bx = (a.size[0] + BX - 1) / BX, by = (a.size[1] + BY - 1) / BY, bz = (a.size[2] + BZ - 1) / BZ;
+    using SH = FwdShapeOf<AR>;
+    const int bx = (a.size[0] + BX - 1) / BX, by = (a.size[1] + SH::by - 1) / SH::by, bz = (a.size[2] + BZ - 1) / BZ;
     const uint64_t bricks = (uint64_t)bx * by * bz;
     // split the projection run across CTAs when the volume has too few bricks to fill the GPU
-    const uint64_t target = (uint64_t)dev.sm_count * 3 * 4;
+    const uint64_t target = (uint64_t)dev.sm_count * 3 * (1024 / SH::nt);
     uint32_t splits = 1;
     if (bricks < target && a.n_entries > (uint32_t)G) {
         splits = (uint32_t)std::min<uint64_t>((target + bricks - 1) / bricks, (a.n_entries + G - 1) / G);
@@ -1407,17 +1465,21 @@ cudaError_t launch_forward(const float *vol, uint32_t *sum, const xpr_projdata *
     if (splits == 0) splits = 1;
     if (a.n_entries > 0 && bricks > 0) {
         dim3 grid((unsigned)bricks, splits);
-        const bool list = a.list_mvp != nullptr;
-        if (arith == kFast) {
-            if (list) k_forward_tiled<kFast, true><<<grid, NT, kFwdSmem, s>>>(vol, sum, pd, a, bx, bz);
-            else k_forward_tiled<kFast, false><<<grid, NT, kFwdSmem, s>>>(vol, sum, pd, a, bx, bz);
-        } else {
-            if (list) k_forward_tiled<kStrict, true><<<grid, NT, kFwdSmem, s>>>(vol, sum, pd, a, bx, bz);
-            else k_forward_tiled<kStrict, false><<<grid, NT, kFwdSmem, s>>>(vol, sum, pd, a, bx, bz);
-        }
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
+        if (a.list_mvp != nullptr) k_forward_tiled<AR, true, SH><<<grid, SH::nt, SH::smem, s>>>(vol, sum, pd, a, bx, bz);
+        else k_forward_tiled<AR, false, SH><<<grid, SH::nt, SH::smem, s>>>(vol, sum, pd, a, bx, bz);
+        return cudaGetLastError();
     }
+    return cudaSuccess;
+}
+
+cudaError_t launch_forward(const float *vol, uint32_t *sum, const xpr_projdata *pd, const LaunchArgs &a0, int arith,
+                           int compat_pad, const DeviceInfo &dev, cudaStream_t s)
+{
+    cudaError_t e = prepare_device_kernels();
+    if (e != cudaSuccess) return e;
+    const LaunchArgs &a = a0;
+    e = arith == kFast ? forward_tiled<kFast>(vol, sum, pd, a0, dev, s) : forward_tiled<kStrict>(vol, sum, pd, a0, dev, s);
+    if (e != cudaSuccess) return e;
     if (compat_pad && a.n_entries > 0) {
         const uint64_t n = (uint64_t)a.size[0] * a.size[1] * a.size[2];
         const uint64_t end = n + (32u - n % 32u);
