@@ -94,8 +94,8 @@ MEASURED_TRAFFIC_PER_VOXEL = {
 # executed-work figures of the same captures (profiles/k_*_c2slab.md): issue-active share,
 # l1tex (shared-memory pipe) throughput and thread instructions per (voxel, projection) pair
 MEASURED_PROFILE = {
-    "strict": {"forward": {"issue_active_pct": 79.6, "l1tex_pct": 71.3, "fma_pipe_pct": 48.8,
-                           "thread_inst_per_pair": 20.7},
+    "strict": {"forward": {"issue_active_pct": 71.5, "l1tex_pct": 69.3, "fma_pipe_pct": 47.6,
+                           "thread_inst_per_pair": 17.7, "shared_atomic_replay_pct": 48.9},
                "backward": {"issue_active_pct": 66.2, "l1tex_pct": 49.7, "fma_pipe_pct": 62.9,
                             "thread_inst_per_pair": 15.5},
                "source": "ncu --set full, c2 geometry 256-layer slab: profiles/k_forward_tiled_strict_c2slab.md, "
@@ -423,7 +423,7 @@ def cpu_reference_step_factory(cfg, seconds_target, max_layers=REF_SAMPLE_LAYERS
         dt_full, _ = run(Hv)
         reps = int(max(1, round(seconds_target / max(dt_full, 1e-3))))
     info = {"kind": kind, "cores": os.cpu_count(), "layers": layers, "W": W, "Hv": Hv, "Pc": Pc, "reps": reps}
-    if not whole and max_layers <= 8:
+    if not whole and max_layers <= 16:
         info["probe_s"], _ = run(layers)  # a timing probe of the thin slab
     return (lambda: run(layers, reps)), info
 
@@ -448,13 +448,19 @@ def run_reference(args, cfg, rank, world):
               "--config c2)" % args.config})
         return 0
     # the cpu_baseline sample (whole small grids once per step; else the central 128-layer slab,
-    # thinned to no fewer than 64 layers if the whole run would take over about four minutes)
+    # thinned to no fewer than 64 layers only if the whole run would take over about five
+    # minutes).  A step costs a fixed part (the error step over the whole detector, thread
+    # start-up) plus a part per layer; probes of 8 and 16 layers separate the two.
     n = max(1, args.steps + args.warmup)
     _, probe_info = cpu_reference_step_factory(cfg, 0.0, max_layers=8)
     layers = REF_SAMPLE_LAYERS
     if probe_info["layers"] < probe_info["Hv"]:
         t8 = probe_info["probe_s"]
-        layers = int(max(64, min(REF_SAMPLE_LAYERS, 8 * 240.0 / n / max(t8, 1e-3))))
+        t16 = cpu_reference_step_factory(cfg, 0.0, max_layers=16)[1]["probe_s"]
+        per_layer = max(t16 - t8, 1e-4) / 8.0
+        fixed = max(t8 - 8.0 * per_layer, 0.0)
+        if n * (fixed + per_layer * REF_SAMPLE_LAYERS) > 300.0:
+            layers = int(max(64, (300.0 / n - fixed) / per_layer))
     step, info = cpu_reference_step_factory(cfg, 0.0, max_layers=layers)
     for _ in range(args.warmup):
         step()
@@ -898,7 +904,9 @@ def run_serving(args, cfg, rank, world, local):
         span = max(i.done_s for i in infos) - min(i.submit_s for i in infos)
         st = srv.stats()
         srv.close()
-        return {"ok": ok, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+        failed = [i for i in infos if i.state != DONE]
+        return {"ok": ok, "failed": len(failed), "errors": sorted({int(i.error) for i in failed}),
+                "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                 "mean_s": float(lat.mean()), "gups": total_pairs / span / 1e9, "makespan_s": span,
                 "ticks": int(st.ticks), "peak_device_gb": st.peak_bytes / 1e9}
 

@@ -257,7 +257,8 @@ typedef struct xpr_request_info {
     int32_t error;                /* XPR_ERR_* of a failed request */
     double submit_s, admit_s, done_s;  /* seconds since the server started */
     uint64_t pairs;               /* voxel x projection pairs of the whole reconstruction */
-    uint64_t device_bytes;        /* device memory held while resident */
+    uint64_t device_bytes;        /* peak device memory held (the admission charge: the resident
+                                     reconstruction plus its raw images until it joins the batch) */
 } xpr_request_info;
 
 typedef struct xpr_serve_stats {

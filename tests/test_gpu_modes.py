@@ -271,3 +271,46 @@ def test_simulation_matches_oracle(tmp_path):
             got = read_tiff(str(tmp_path / "sim" / ("p_%010d.tif" % (sit + k * S))))
             exp = (sums[k * W * H:(k + 1) * W * H].astype(np.float32) / np.float32(4194304.0)).reshape(H, W)
             np.testing.assert_array_equal(got.view(np.uint32), exp.view(np.uint32))
+
+
+def write_layers(dirpath, vol, H, W):
+    """A volume (H layers of W x W, y outermost) as the layer_%05d.tif stack a run saves."""
+    L = _lib.lib()
+    L.xpr_tiff_write.argtypes = [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32]
+    os.makedirs(dirpath, exist_ok=True)
+    v = vol.reshape(H, W, W)
+    for l in range(H):
+        layer = np.ascontiguousarray(v[l])
+        assert L.xpr_tiff_write(os.path.join(dirpath, "layer_%05d.tif" % l).encode(), layer.ctypes.data, W, W) == 0
+
+
+@pytest.mark.parametrize("method", ["naive", "method_1a", "method_1b", "method_1c"])
+def test_resume_continues_the_run(tmp_path, method):
+    """Iterations 0 .. 1 of a run, then iteration 2 resumed from their saved layers
+    (recon.resume, recon.first_iteration 2), equal the uninterrupted 3-iteration run bit for
+    bit: the resumed run takes iteration 2's weight and origin-jitter draws and projects in
+    its first sub-iteration."""
+    raw = raw_images(11)
+    H, W = raw.shape[1:]
+    whole = run_host(config(method, it=3, slab=5), raw)
+    part = run_host(config(method, it=2, slab=5), raw)
+    write_layers(str(tmp_path / "ckpt"), part, H, W)
+    resumed = run_host(config(method, it=3, slab=5, resume=str(tmp_path / "ckpt"), first_iteration=2), raw)
+    assert np.isfinite(whole).mean() > 0.5
+    assert_same_bits(resumed, whole)
+    assert not np.array_equal(part.view(np.uint32), whole.view(np.uint32))  # the last iteration did change it
+
+
+def test_resume_rejects_a_stack_of_another_size(tmp_path):
+    raw = raw_images(12)
+    H, W = raw.shape[1:]
+    write_layers(str(tmp_path / "ckpt"), np.ones((H + 2) * (W + 2) * (W + 2), np.float32), H + 2, W + 2)
+    L = _lib.lib()
+    L.xpr_reconstruct_host.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.c_uint32, C.c_uint32, C.c_void_p,
+                                       C.c_uint64, C.POINTER(C.c_double)]
+    out = np.zeros(W * H * W, np.float32)
+    cfg = config("naive", it=2, resume=str(tmp_path / "ckpt"), first_iteration=1)
+    rc = L.xpr_reconstruct_host(json.dumps(cfg).encode(), np.ascontiguousarray(raw).ctypes.data, raw.shape[0], W, H,
+                                out.ctypes.data, out.size, C.byref(C.c_double()))
+    assert rc != 0
+    assert b"layer size mismatch" in L.xpr_last_error()

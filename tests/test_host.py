@@ -83,8 +83,20 @@ def test_parameters_accept_readme_style_json(L):
     assert p["method2"]["overlap_fct"] == 1.0  # parameters.hpp:35 clamps to [0.01, 1]
 
 
+def test_resume_keys_round_trip(L):
+    rc, out = normalize(L, '{"recon": {"it": 4, "resume": "./recon/", "first_iteration": 3}}')
+    assert rc == 0, out
+    r = json.loads(out)["recon"]
+    assert r["resume"] == "./recon/" and r["first_iteration"] == 3
+    rc, out = normalize(L, '{"recon": {"it": 4}}')
+    assert "resume" not in json.loads(out)["recon"]
+
+
 @pytest.mark.parametrize("text", ['{"recon": {"method": "bogus"}}', '{"recon": {"it": "x"}}', '{"recon": ', "[1, 2]",
-                                  '{"detector": {"module_number": 2, "modules": [{}]}}'])
+                                  '{"detector": {"module_number": 2, "modules": [{}]}}',
+                                  '{"recon": {"it": 2, "first_iteration": 2}}',
+                                  '{"recon": {"it": 2, "first_iteration": -1}}',
+                                  '{"recon": {"it": 3, "first_iteration": 1.5}}'])
 def test_bad_parameters_are_rejected(L, text):
     rc, msg = normalize(L, text)
     assert rc == 6, msg  # XPR_ERR_PARAM

@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libxpr.so")
+# XPR_LIB names another build of the same C ABI (a deployment's own copy of the library)
+LIB_PATH = os.environ.get("XPR_LIB") or os.path.join(HERE, "lib", "libxpr.so")
 
 XPR_OK = 0
 # status codes (enum xpr_status)

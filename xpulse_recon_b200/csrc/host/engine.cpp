@@ -327,6 +327,41 @@ struct Engine::Impl {
         return v;
     }
 
+    // recon.resume: layers [y0, y1) of a previous result's stack into dst (W x W each); saved
+    // layers carry the normalisation's (max - min) factor, divided out here
+    void load_layers(const Params &p, float *dst, int64_t y0, int64_t y1)
+    {
+        for (int64_t l = y0; l < y1; ++l) {
+            uint32_t w = 0, h = 0;
+            std::vector<float> layer = tiff_read_f32(layer_path(p.resume, l), &w, &h);
+            if (w != (uint32_t)W || h != (uint32_t)W)
+                throw std::runtime_error("recon.resume: layer size mismatch: " + layer_path(p.resume, l));
+            if (p.normalize)
+                for (auto &v : layer) v = v / (nmax - nmin);
+            std::memcpy(dst + (size_t)(l - y0) * W * W, layer.data(), sizeof(float) * W * W);
+        }
+    }
+
+    // recon.first_iteration k: iteration k's weight (the schedule's float products) and the
+    // origin-jitter draws of iterations 0 .. k - 1 taken and dropped
+    float start_weight(const Params &p) const
+    {
+        float w = p.weight;
+        for (int64_t k = 0; k < p.first_iteration; ++k) w *= p.weight_factor;
+        return w;
+    }
+    void skip_jitter(const Params &p, const xpr_geom_out &go)
+    {
+        float o[3];
+        for (int64_t k = 0; k < p.first_iteration * S; ++k) jittered_origin(go, o);
+    }
+    // the reference skips the very first forward (the uniform volume's sums are preset); a
+    // resumed volume is not uniform, so every sub-iteration of a resumed run projects
+    static bool skips_forward(const Params &p, int64_t mit, int64_t sit)
+    {
+        return mit == 0 && sit == 0 && p.resume.empty();
+    }
+
     void save_layers(const Params &p, const float *vol, int64_t y0, int64_t y1)
     {
         std::vector<float> layer((size_t)(W * W));
@@ -424,15 +459,22 @@ void Engine::reconstruct()
         check(xpr_upload(d.ctx, pd.p, spd.data(), spd.size() * PDB, d.comp->v()), "upload");
         check(xpr_fill_u32(d.ctx, vol.p, 0x3f800000u, nvol, d.comp->v()), "fill");          // :59
         check(xpr_fill_u32(d.ctx, sum.p, 1u << 22, Pc * WH, d.comp->v()), "fill");           // :60
+        if (!p.resume.empty()) {
+            std::vector<float> init(N);
+            d.load_layers(p, init.data(), 0, Hv);
+            check(xpr_upload(d.ctx, vol.p, init.data(), N * 4, d.comp->v()), "upload");
+            d.comp->sync();
+        }
         std::cout << "Executing reconstruction..." << std::flush;
         const double t1 = now();
-        float weight = p.weight;
-        for (int64_t mit = 0; mit < p.it; ++mit) {
+        float weight = d.start_weight(p);
+        d.skip_jitter(p, go_);
+        for (int64_t mit = p.first_iteration; mit < p.it; ++mit) {
             for (int64_t sit = 0; sit < S; ++sit) {
                 d.jittered_origin(go_, origin);
                 xpr_launch L = d.launch(0, (int32_t)Hv, origin, go_.vx, (uint32_t)d.Hd, 0, (uint32_t)Pc,
                                         p.compat_pad ? 1 : 0);
-                const bool first = (mit == 0 && sit == 0);
+                const bool first = Impl::skips_forward(p, mit, sit);
                 check(xpr_subiteration(d.ctx, vol.as<float>(), sum.as<uint32_t>(),
                                        img.at((uint64_t)sit * Pc * WH * d.iesize), d.idt, sep ? ratio.p : sum.p,
                                        d.rdt, (const xpr_projdata *)pd.at((uint64_t)sit * Pc * M * PDB),
@@ -505,6 +547,7 @@ void Engine::reconstruct()
         float *hv = hvol.as<float>();
 #pragma omp parallel for schedule(static) num_threads(8)
         for (int64_t i = 0; i < (int64_t)N; ++i) hv[i] = init;
+        if (!p.resume.empty()) d.load_layers(p, hv, 0, Hv);
         if (!lplh)  // reconstruction_lpla.hpp:243
             check(xpr_fill_u32(d.ctx, sum.p, 1u << 22, (uint64_t)slots * WH, d.comp->v()), "fill");
         double t1 = 0.0;
@@ -518,12 +561,13 @@ void Engine::reconstruct()
             DevBuf sb(d.ctx, (uint64_t)slab * layer_bytes);
             std::cout << "Executing reconstruction..." << std::flush;
             t1 = now();
-            float weight = p.weight;
+            float weight = d.start_weight(p);
+            d.skip_jitter(p, go_);
             const int64_t nslab = (Hv + slab - 1) / slab;
-            for (int64_t mit = 0; mit < p.it; ++mit) {
+            for (int64_t mit = p.first_iteration; mit < p.it; ++mit) {
                 for (int64_t sit = 0; sit < S; ++sit) {
                     d.jittered_origin(go_, origin);
-                    const bool first = (mit == 0 && sit == 0);
+                    const bool first = Impl::skips_forward(p, mit, sit);
                     check(xpr_upload(d.ctx, img.p, himg.at((uint64_t)sit * slots * WH * d.iesize),
                                      (uint64_t)Pc * WH * d.iesize, d.comp->v()), "upload");
                     const void *pdp = pd.at((uint64_t)sit * Pc * M * PDB);
@@ -629,11 +673,12 @@ void Engine::reconstruct()
             };
             std::cout << "Executing reconstruction..." << std::flush;
             t1 = now();
-            float weight = p.weight;
-            for (int64_t mit = 0; mit < p.it; ++mit) {
+            float weight = d.start_weight(p);
+            d.skip_jitter(p, go_);
+            for (int64_t mit = p.first_iteration; mit < p.it; ++mit) {
                 for (int64_t sit = 0; sit < S; ++sit) {
                     d.jittered_origin(go_, origin);
-                    const bool first = (mit == 0 && sit == 0);
+                    const bool first = Impl::skips_forward(p, mit, sit);
                     const int64_t nimg = lplh ? d.angles_in(sit) : Pc;
                     check(xpr_upload(d.ctx, img.p, himg.at((uint64_t)sit * slots * WH * d.iesize),
                                      (uint64_t)nimg * WH * d.iesize, d.comp->v()), "upload");
@@ -741,8 +786,18 @@ void Engine::reconstruct()
             DevBuf ratio = sep ? DevBuf(d.ctx, (uint64_t)Pc * cw * d.rsize) : DevBuf();
             check(xpr_fill_u32(d.ctx, slab.p, 0x3f800000u, (uint64_t)ny * W * W, d.comp->v()), "fill");
             check(xpr_fill_u32(d.ctx, sum.p, 1u << 22, (uint64_t)Pc * cw, d.comp->v()), "fill");
-            float weight = p.weight;
-            for (int64_t mit = 0; mit < p.it; ++mit) {
+            if (!p.resume.empty()) {
+                // the chunk's layers with their padding from the stack (a continuous run's
+                // padding layers are the chunk's own and are not saved, so a resumed chunk
+                // starts its padding from the neighbouring chunks' saved layers)
+                std::vector<float> init((size_t)ny * W * W);
+                d.load_layers(p, init.data(), y0, y0 + ny);
+                check(xpr_upload(d.ctx, slab.p, init.data(), init.size() * 4, d.comp->v()), "upload");
+                d.comp->sync();
+            }
+            float weight = d.start_weight(p);
+            d.skip_jitter(p, go_);
+            for (int64_t mit = p.first_iteration; mit < p.it; ++mit) {
                 for (int64_t sit = 0; sit < S; ++sit) {
                     // the chunk's detector-row window of this sub-iteration's images
                     for (int64_t k = 0; k < Pc; ++k)
@@ -752,7 +807,7 @@ void Engine::reconstruct()
                     d.jittered_origin(go_, origin);
                     xpr_launch L = d.launch((int32_t)y0, (int32_t)(y0 + ny), origin, go_.vx, (uint32_t)rows,
                                             (int32_t)c.iOffset, (uint32_t)Pc, 0);
-                    const bool first = (mit == 0 && sit == 0);
+                    const bool first = Impl::skips_forward(p, mit, sit);
                     check(xpr_subiteration(d.ctx, slab.as<float>(), sum.as<uint32_t>(), img.p, d.idt,
                                            sep ? ratio.p : sum.p, d.rdt,
                                            (const xpr_projdata *)pd.at((uint64_t)sit * Pc * M * PDB), (uint32_t)(Pc * M),

@@ -114,6 +114,12 @@ Params params_from_json(const json::Value &root)
         if (p.geometry != "fp32" && p.geometry != "fp64") throw std::runtime_error("recon.geometry must be fp32|fp64");
     });
     opt(r, "compat_pad", [&](const json::Value &v) { p.compat_pad = boolean(v, "compat_pad"); });
+    opt(r, "resume", [&](const json::Value &v) { p.resume = str(v, "resume"); });
+    opt(r, "first_iteration", [&](const json::Value &v) {
+        const double k = num(v, "first_iteration");
+        if (k < 0.0 || k != (double)(int64_t)k) throw std::runtime_error("recon.first_iteration must be an integer >= 0");
+        p.first_iteration = (int64_t)k;
+    });
     opt(r, "mem_cap", [&](const json::Value &v) {
         p.mem_cap = v.type == json::Value::String ? parse_bytes(v.str) : (uint64_t)num(v, "mem_cap");
     });
@@ -179,6 +185,7 @@ Params params_from_json(const json::Value &root)
     if (p.overlap_fct < 0.01f) p.overlap_fct = 0.01f;
     if (p.heli_step < 1.0f) p.heli_step = 1.0f;
     if (p.it < 1 || p.sit < 1) throw std::runtime_error("recon.it and recon.sit must be >= 1");
+    if (p.first_iteration >= p.it) throw std::runtime_error("recon.first_iteration must be below recon.it");
     if (p.module_number < 1) throw std::runtime_error("detector.module_number must be >= 1");
     if (!p.modules.empty() && (int64_t)p.modules.size() != p.module_number)
         throw std::runtime_error("detector.modules must list module_number entries");
@@ -212,6 +219,8 @@ std::string params_to_json(const Params &p)
     if (p.seed_set) o << ",\"seed\":" << p.seed;
     o << ",\"arith\":\"" << p.arith << "\",\"storage\":\"" << p.storage << "\"";
     if (!p.image_storage.empty()) o << ",\"image_storage\":\"" << p.image_storage << "\"";
+    if (!p.resume.empty()) o << ",\"resume\":" << json::quote(p.resume);
+    if (p.first_iteration > 0) o << ",\"first_iteration\":" << p.first_iteration;
     o << ",\"geometry\":\"" << p.geometry
       << "\",\"compat_pad\":" << b(p.compat_pad) << ",\"mem_cap\":" << p.mem_cap << ",\"device\":" << p.device
       << ",\"slab\":" << p.slab << ",\"slab_cache\":" << p.slab_cache << "}";

@@ -18,6 +18,14 @@
 //   recon.slab           layers per streamed y-slab in method_1a/1b/1c (0: as many as fit)
 //   recon.slab_cache     slabs method_1b/1c keep on the device (0: as many as the memory holds)
 //   recon.images_preproc alias of recon.normalize (the README's name for it)
+//   recon.resume         directory of a previous result's layer_%05d.tif stack: the initial
+//                        volume instead of the uniform one (every sub-iteration runs its
+//                        forward; with recon.normalize the layers are divided by the images'
+//                        max - min, the inverse of the scaling they were saved with)
+//   recon.first_iteration  k: the run performs iterations k .. it - 1 of the schedule, with
+//                        iteration k's weight (weight * weight_factor^k) and origin-jitter
+//                        draws; with recon.resume on the result of iterations 0 .. k - 1 it
+//                        continues that run bit for bit (naive, method_1a / 1b / 1c)
 //   detector.modules[]   per-module {offset_x, offset_y, offset_z, roll, pitch, yaw}
 //                        (the reference's commented-out global_parameters.hpp:38-44, 51)
 #pragma once
@@ -78,6 +86,8 @@ struct Params {
     std::string image_storage;  // empty: as storage
     std::string geometry = "fp32";
     bool compat_pad = false;
+    std::string resume;  // empty: the uniform initial volume
+    int64_t first_iteration = 0;
     uint64_t mem_cap = 0;
     int device = 0;
     int64_t slab = 0;

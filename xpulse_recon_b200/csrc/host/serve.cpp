@@ -59,6 +59,9 @@ struct Request {
     uint64_t N = 0, npix = 0, bytes = 0, pairs = 0;
     // device
     void *arena = nullptr;
+    float *raw_dev = nullptr;       // the raw images on the device, until the compute thread preprocesses them
+    uint64_t raw_bytes = 0;
+    int64_t raw_images = 0;         // images uploaded: all P when normalising (min / max over all), else S * Pc
     xpr::PlannedProblem pp;
     cudaEvent_t ready = nullptr, done_ev = nullptr;
     uint32_t step = 0;
@@ -89,14 +92,13 @@ struct xpr_server {
     xpr_serve_stats stats{};
     // io resources
     cudaStream_t io = nullptr, comp = nullptr, dl = nullptr;
-    void *pinned[2] = {nullptr, nullptr};
+    void *pinned[2] = {nullptr, nullptr};     // upload ring for callers' pageable images
     void *dl_pinned[2] = {nullptr, nullptr};  // download ring of dl_bytes per chunk
     size_t dl_bytes = 0;
     cudaEvent_t dl_ev[2] = {nullptr, nullptr};
-    float *dstage[2] = {nullptr, nullptr};
     cudaEvent_t chunk_ev[2] = {nullptr, nullptr};
     size_t chunk_bytes = 0;
-    float *minmax = nullptr;  // device {min, max} of the request being admitted
+    float *minmax = nullptr;  // device {min, max} of the request being prepared (compute thread)
     // compute resources
     uint32_t *tickets = nullptr;
     char *items_host[2] = {nullptr, nullptr};
@@ -125,15 +127,11 @@ bool ensure_chunks(xpr_server *s, size_t bytes)
     for (int b = 0; b < 2; ++b) {
         if (s->chunk_ev[b]) cudaEventSynchronize(s->chunk_ev[b]);
         if (s->pinned[b]) cudaFreeHost(s->pinned[b]);
-        if (s->dstage[b]) cudaFree(s->dstage[b]);
         s->pinned[b] = nullptr;
-        s->dstage[b] = nullptr;
     }
     s->chunk_bytes = 0;
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < 2; ++b)
         if (cudaHostAlloc(&s->pinned[b], bytes, cudaHostAllocDefault) != cudaSuccess) return false;
-        if (cudaMalloc((void **)&s->dstage[b], bytes) != cudaSuccess) return false;
-    }
     // the download ring keeps the size it was made with (the download thread owns it)
     for (int b = 0; b < 2 && !s->dl_pinned[b]; ++b) {
         if (cudaHostAlloc(&s->dl_pinned[b], bytes, cudaHostAllocDefault) != cudaSuccess) return false;
@@ -143,33 +141,55 @@ bool ensure_chunks(xpr_server *s, size_t bytes)
     return true;
 }
 
-// Runs `per_chunk(first image, images in chunk, device chunk)` over the request's images
-// [0, n_img) staged through the pinned ring: host copy into pinned memory, one
-// cudaMemcpyAsync to the device chunk, then the chunk's kernels on the io stream.
-template <typename F>
-void stream_images(xpr_server *s, Request *r, int64_t n_img, F &&per_chunk)
+// The request's raw images [0, raw_images) to its device buffer on the io stream: one copy
+// from a page-locked caller buffer, else through the pinned ring (host copy, then a copy
+// to the device, the two overlapped).  Only copies run here: the io stream carries no
+// kernel, so the uploads never wait for the compute thread's persistent launches, which
+// hold every SM while a tick runs.
+void upload_raw(xpr_server *s, Request *r)
 {
-    const size_t img_bytes = (size_t)r->W * r->H * sizeof(float);
-    if (!ensure_chunks(s, std::max(kChunkBytes, img_bytes))) throw std::runtime_error("pinned staging allocation");
-    const int64_t per = (int64_t)(s->chunk_bytes / img_bytes);
+    const size_t total = (size_t)r->raw_images * r->W * r->H * sizeof(float);
+    if (r->raw_pinned) {
+        check_cuda(cudaMemcpyAsync(r->raw_dev, r->raw, total, cudaMemcpyHostToDevice, s->io), "upload");
+        return;
+    }
     int b = 0;
-    for (int64_t i0 = 0; i0 < n_img; i0 += per, b ^= 1) {
-        const int64_t n = std::min(per, n_img - i0);
+    for (size_t off = 0; off < total; off += s->chunk_bytes, b ^= 1) {
+        const size_t n = std::min(s->chunk_bytes, total - off);
         check_cuda(cudaEventSynchronize(s->chunk_ev[b]), "staging");
-        const float *src = r->raw + (size_t)i0 * r->W * r->H;
-        if (!r->raw_pinned) {
-            par_memcpy(s->pinned[b], src, (size_t)n * img_bytes);
-            src = (const float *)s->pinned[b];
-        }
-        check_cuda(cudaMemcpyAsync(s->dstage[b], src, (size_t)n * img_bytes, cudaMemcpyHostToDevice, s->io), "upload");
-        per_chunk(i0, n, s->dstage[b]);
+        par_memcpy(s->pinned[b], (const char *)r->raw + off, n);
+        check_cuda(cudaMemcpyAsync((char *)r->raw_dev + off, s->pinned[b], n, cudaMemcpyHostToDevice, s->io),
+                   "upload");
         check_cuda(cudaEventRecord(s->chunk_ev[b], s->io), "staging");
     }
 }
 
+// The request's device memory (the arena and the raw-image buffer) from the stream-ordered
+// pool; on failure neither is kept.  Finished requests free their memory in stream order
+// (download and compute streams), so a failed allocation waits for those frees to run and
+// tries once more.
+cudaError_t alloc_request(xpr_server *s, Request *r)
+{
+    cudaError_t e = cudaSuccess;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        e = cudaMallocAsync(&r->arena, r->bytes, s->io);
+        if (e == cudaSuccess) e = cudaMallocAsync((void **)&r->raw_dev, r->raw_bytes, s->io);
+        if (e == cudaSuccess) return e;
+        cudaGetLastError();  // an allocation failure is not sticky; clear it
+        if (r->arena) cudaFreeAsync(r->arena, s->io);
+        if (r->raw_dev) cudaFreeAsync(r->raw_dev, s->io);
+        r->arena = nullptr;
+        r->raw_dev = nullptr;
+        if (e != cudaErrorMemoryAllocation) break;
+        cudaStreamSynchronize(s->dl);
+        cudaStreamSynchronize(s->comp);
+        cudaStreamSynchronize(s->io);
+    }
+    return e;
+}
+
 void upload_request(xpr_server *s, Request *r)
 {
-    check_cuda(cudaMallocAsync(&r->arena, r->bytes, s->io), "cudaMallocAsync");
     char *q = (char *)r->arena;
     auto take = [&](uint64_t bytes) {
         char *p = q;
@@ -181,28 +201,9 @@ void upload_request(xpr_server *s, Request *r)
     xpr_projdata *pd = (xpr_projdata *)take(sizeof(xpr_projdata) * r->pd_sub.size());
     uint32_t *sums = (uint32_t *)take(4 * r->npix);
     void *ratio = take(s->esize * r->npix);
-    check_cuda(xpr::launch_fill_u32(vol, kOneBits, r->N, *s->di, s->io), "fill");  // reconstruction_n.hpp:59
     check_cuda(cudaMemcpyAsync(pd, r->pd_sub.data(), sizeof(xpr_projdata) * r->pd_sub.size(), cudaMemcpyHostToDevice,
                                s->io), "projdata upload");
-    const uint64_t WH = (uint64_t)r->W * r->H;
-    const int64_t used = r->S * r->Pc;  // acquisitions s + k * S, k < Pc (geometry.hpp:306-327)
-    if (r->p.normalize) {  // data_loader.hpp:48-66: min / max over the std::isnormal values
-        const float init[2] = {3.402823466e38f, 1.175494351e-38f};
-        check_cuda(cudaMemcpyAsync(s->minmax, init, sizeof(init), cudaMemcpyHostToDevice, s->io), "minmax");
-        check_cuda(cudaStreamSynchronize(s->io), "minmax");
-        stream_images(s, r, r->P, [&](int64_t, int64_t n, float *d) {
-            check_cuda(xpr::launch_minmax(d, (uint64_t)n * WH, s->minmax, *s->di, s->io), "minmax");
-        });
-    }
-    stream_images(s, r, used, [&](int64_t i0, int64_t n, float *d) {
-        for (int64_t j = i0; j < i0 + n; ++j) {
-            const int64_t slot = (j % r->S) * r->Pc + j / r->S;
-            check_cuda(xpr::launch_preprocess(d + (j - i0) * WH, images + (size_t)slot * WH * s->iesize,
-                                              s->opts.image_storage, WH, r->p.normalize ? 1 : 0, s->minmax,
-                                              r->p.mlog ? 1 : 0, *s->di, s->io),
-                       "preprocess");
-        }
-    });
+    upload_raw(s, r);
     xpr_batch_problem bp{};
     bp.vol = vol;
     bp.images = images;
@@ -306,25 +307,47 @@ void io_loop(xpr_server *s)
         if (!s->queue.empty()) {
             Request *r = s->queue.front();
             const uint64_t resident = s->active.size() + s->ready.size();
-            const bool fits = s->bytes_in_use + r->bytes <= s->opts.mem_budget;
+            const bool fits = s->bytes_in_use + r->bytes + r->raw_bytes <= s->opts.mem_budget;
             const bool slot = s->opts.max_active == 0 || resident < s->opts.max_active;
             if (fits && slot) {
                 s->queue.pop_front();
-                s->bytes_in_use += r->bytes;
+                s->bytes_in_use += r->bytes + r->raw_bytes;
                 s->peak_bytes = std::max(s->peak_bytes, s->bytes_in_use);
                 r->admit_s = now_s(s->t0);
+                const uint64_t others = s->bytes_in_use - (r->bytes + r->raw_bytes);
                 lk.unlock();
+                const cudaError_t ae = alloc_request(s, r);
                 int err = 0;
-                try {
-                    upload_request(s, r);
-                } catch (const std::exception &) {
+                if (ae == cudaSuccess) {
+                    try {
+                        upload_request(s, r);
+                    } catch (const std::exception &) {
+                        err = XPR_ERR_CUDA;
+                    }
+                } else if (ae != cudaErrorMemoryAllocation) {
                     err = XPR_ERR_CUDA;
                 }
                 lk.lock();
+                if (ae == cudaErrorMemoryAllocation) {
+                    // the device holds less than the budget allows (memory of other users of
+                    // the device, fragmentation): while other requests hold memory, the
+                    // request waits at the head of the queue for one of them to release
+                    // some; alone on the server it can never fit
+                    s->bytes_in_use -= r->bytes + r->raw_bytes;
+                    if (s->bytes_in_use > 0) {
+                        s->queue.push_front(r);
+                        if (s->bytes_in_use >= others) s->cv_io.wait(lk);  // else some was released meanwhile
+                        continue;
+                    }
+                    err = XPR_ERR_OOM;
+                    s->bytes_in_use += r->bytes + r->raw_bytes;  // released below with the failure
+                }
                 if (err) {
                     if (r->arena) cudaFreeAsync(r->arena, s->io);
+                    if (r->raw_dev) cudaFreeAsync(r->raw_dev, s->io);
                     r->arena = nullptr;
-                    s->bytes_in_use -= r->bytes;
+                    r->raw_dev = nullptr;
+                    s->bytes_in_use -= r->bytes + r->raw_bytes;
                     r->state = XPR_REQ_FAILED;
                     r->error = err;
                     r->done_s = now_s(s->t0);
@@ -343,6 +366,28 @@ void io_loop(xpr_server *s)
 }
 
 // ---------------------------------------------------------------------- compute thread
+// A request joining the batch, on the compute stream ahead of its first tick: the volume
+// set to 1.0 (reconstruction_n.hpp:59), then the -log / normalise preprocessing
+// (data_loader.hpp:48-101; min / max over every image when normalising) of its raw images
+// into the storage type in subset-major order, in one launch; the raw buffer is released.
+cudaError_t prepare_on_device(xpr_server *s, Request *r)
+{
+    const uint64_t WH = (uint64_t)r->W * r->H;
+    cudaError_t e = xpr::launch_fill_u32(r->pp.p.vol, kOneBits, r->N, *s->di, s->comp);
+    if (e == cudaSuccess && r->p.normalize) {
+        e = xpr::launch_fill_u32(s->minmax, 0x7f7fffffu, 1, *s->di, s->comp);  // FLT_MAX (data_loader.hpp:12-13)
+        if (e == cudaSuccess) e = xpr::launch_fill_u32(s->minmax + 1, 0x00800000u, 1, *s->di, s->comp);  // FLT_MIN
+        if (e == cudaSuccess) e = xpr::launch_minmax(r->raw_dev, (uint64_t)r->P * WH, s->minmax, *s->di, s->comp);
+    }
+    if (e == cudaSuccess)
+        e = xpr::launch_preprocess_reorder(r->raw_dev, const_cast<void *>(r->pp.p.images), s->opts.image_storage, WH,
+                                           (uint32_t)(r->S * r->Pc), (uint32_t)r->S, (uint32_t)r->Pc,
+                                           r->p.normalize ? 1 : 0, s->minmax, r->p.mlog ? 1 : 0, *s->di, s->comp);
+    const cudaError_t f = cudaFreeAsync(r->raw_dev, s->comp);
+    r->raw_dev = nullptr;
+    return e != cudaSuccess ? e : f;
+}
+
 void compute_loop(xpr_server *s)
 {
     xpr::context_device(s->ctx);
@@ -350,12 +395,23 @@ void compute_loop(xpr_server *s)
     uint64_t tick = 0;
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
-        // join the requests whose upload completed
+        // join the requests whose upload completed (preprocessed on this stream first)
         for (auto it = s->ready.begin(); it != s->ready.end();) {
-            if (cudaEventQuery((*it)->ready) == cudaSuccess) {
-                (*it)->state = XPR_REQ_ACTIVE;
-                s->active.push_back(*it);
+            Request *r = *it;
+            if (cudaEventQuery(r->ready) == cudaSuccess) {
                 it = s->ready.erase(it);
+                const cudaError_t e = prepare_on_device(s, r);
+                s->bytes_in_use -= r->raw_bytes;
+                s->cv_io.notify_all();  // the raw images' memory released: admission may proceed
+                if (e != cudaSuccess) {
+                    r->error = XPR_ERR_CUDA;
+                    cudaEventRecord(r->done_ev, s->comp);
+                    s->finishing.push_back(r);
+                    s->cv_dl.notify_all();
+                    continue;
+                }
+                r->state = XPR_REQ_ACTIVE;
+                s->active.push_back(r);
             } else {
                 ++it;
             }
@@ -486,6 +542,8 @@ bool prepare_request(xpr_server *s, Request *r, std::string *msg)
     auto al = [](uint64_t b) { return (b + 255) & ~255ull; };
     r->bytes = al(4 * r->N) + al(s->iesize * r->npix * r->S) + al(sizeof(xpr_projdata) * r->pd_sub.size()) +
                al(4 * r->npix) + al(s->esize * r->npix);
+    r->raw_images = r->p.normalize ? r->P : r->S * r->Pc;
+    r->raw_bytes = al((uint64_t)r->raw_images * r->W * r->H * sizeof(float));
     r->pairs = r->N * (uint64_t)r->Pc * (uint64_t)r->S * (uint64_t)r->p.it;
     return true;
 }
@@ -494,7 +552,6 @@ void release(xpr_server *s)
 {
     for (int b = 0; b < 2; ++b) {
         if (s->pinned[b]) cudaFreeHost(s->pinned[b]);
-        if (s->dstage[b]) cudaFree(s->dstage[b]);
         if (s->chunk_ev[b]) cudaEventDestroy(s->chunk_ev[b]);
         if (s->items_host[b]) cudaFreeHost(s->items_host[b]);
         if (s->items_dev[b]) cudaFree(s->items_dev[b]);
@@ -522,7 +579,7 @@ void fill_info(const Request *r, xpr_request_info *info)
     info->admit_s = r->admit_s;
     info->done_s = r->done_s;
     info->pairs = r->pairs;
-    info->device_bytes = r->bytes;
+    info->device_bytes = r->bytes + r->raw_bytes;  // the peak: the raw images are held until the request joins
 }
 
 }  // namespace
@@ -596,9 +653,9 @@ int xpr_serve_submit(xpr_server *s, const char *json, const float *raw, int64_t 
     if (r->N > vol_cap)
         return xpr::set_last_error(XPR_ERR_INVALID, "xpr_serve_submit: vol_out holds %llu floats, %llu needed",
                                    (unsigned long long)vol_cap, (unsigned long long)r->N);
-    if (r->bytes > s->opts.mem_budget)
+    if (r->bytes + r->raw_bytes > s->opts.mem_budget)
         return xpr::set_last_error(XPR_ERR_CAP, "xpr_serve_submit: the request needs %llu device bytes, the budget "
-                                                "is %llu", (unsigned long long)r->bytes,
+                                                "is %llu", (unsigned long long)(r->bytes + r->raw_bytes),
                                    (unsigned long long)s->opts.mem_budget);
     if (!xpr::context_device(s->ctx)) return XPR_ERR_INVALID;
     auto pinned = [](const void *p) {

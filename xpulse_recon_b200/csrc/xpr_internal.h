@@ -56,6 +56,11 @@ cudaError_t launch_error(const void *images, int image_dtype, uint32_t *sum, voi
                          float weight, int mode, int zero_sum, double *residual, const DeviceInfo &dev,
                          cudaStream_t s);
 cudaError_t launch_minmax(const float *images, uint64_t n, float *minmax, const DeviceInfo &dev, cudaStream_t s);
+// images [0, n_img) of wh pixels (acquisition order) preprocessed into subset-major slots
+// (j mod S) * Pc + j / S of `out`
+cudaError_t launch_preprocess_reorder(const float *images, void *out, int out_dtype, uint64_t wh, uint32_t n_img,
+                                      uint32_t S, uint32_t Pc, int normalize, const float *minmax, int mlog,
+                                      const DeviceInfo &dev, cudaStream_t s);
 cudaError_t launch_preprocess(const float *images, void *out, int out_dtype, uint64_t n, int normalize,
                               const float *minmax, int mlog, const DeviceInfo &dev, cudaStream_t s);
 cudaError_t launch_fill_u32(void *dst, uint32_t value, uint64_t count, const DeviceInfo &dev, cudaStream_t s);

@@ -50,6 +50,8 @@ constexpr int BZ = 32;          // forward brick extent along z
 constexpr int NT = 256;         // threads per CTA (8 warps)
 constexpr int G = 4;            // projections whose tiles are in flight together
 constexpr int TILE_CAP = 1024;  // pixels per shared-memory tile
+constexpr int MCAP = 32;        // forward: projections whose metadata a CTA prepares at once
+static_assert(MCAP % G == 0 && MCAP / G <= NT / 32, "one group of G projections per warp");
 constexpr int VSTRIDE = 132;    // padded row stride (words) of the brick value array: 32 x-positions of four
                                 // layers interleaved, + 4 (128-bit reads bank-conflict free both ways)
 constexpr int BWD_BY = 16;      // backward column length along y
@@ -281,6 +283,12 @@ __device__ __forceinline__ void tilted_pair(float py0, float py1, float4 cu, flo
 // Register-pair forms: the operands are 64-bit pairs {lo, hi}, and values that stay packed
 // across a column (the y positions, the column constants) are paired once, not per
 // instruction; the backward's walk uses these.
+// an add to a shared-memory word by its 32-bit shared-window address
+__device__ __forceinline__ void red_shared_add(uint32_t saddr, uint32_t v)
+{
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(saddr), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ uint64_t f2pack(float lo, float hi)
 {
     uint64_t d;
@@ -404,9 +412,12 @@ __device__ __forceinline__ void tilted_pair(uint64_t P, const Packed &k, uint64_
 // C_u, C_v, C_w = fma(c.x, px, c.w) + c.z * pz; same calls and return value.  Two forms
 // of the same arithmetic: y positions as floats (this one, the forward's: measured faster
 // there) or in register pairs (the next one, the backward's: measured faster there).
+// isc / ib: f receives the target index as idx * isc + ib (mod 2^32); a shared-memory tile
+// passes its element size and its shared-window address, so the walk's one multiply-add
+// per voxel forms the atomic's address (isc = 1, ib = 0: the plain index).
 template <int LEN, typename F>
 __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a, float Cu, float Cv, float Cw,
-                                         const float (&py)[LEN], F &&f)
+                                         const float (&py)[LEN], F &&f, uint32_t isc = 1u, uint32_t ib = 0u)
 {
     const float4 cu = M.cu, cv = M.cv, cw = M.cw;
     const uint4 tgt = M.tgt;
@@ -419,7 +430,8 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
         const uint32_t Kv = tgt.y - fb.z * pitch;
         if (M.flags.z) {
             const float rw = __frcp_rn(Cw);
-            const uint32_t K = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x) + Kv;
+            const uint32_t K = (fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x) + Kv) * isc + ib;
+            const uint32_t pitchS = pitch * isc;
             const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
             static_assert(LEN % 2 == 0, "columns are walked two voxels at a time");
 #pragma unroll
@@ -427,8 +439,8 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
                 float y0, y1, b0, b1;
                 fma_rn2(y0, y1, py[k], py[k + 1], Qv, Rv);
                 add_rz2(b0, b1, y0, y1, 8388608.0f);
-                f(std::true_type{}, k, true, __float_as_uint(b0) * pitch + K);
-                f(std::true_type{}, k + 1, true, __float_as_uint(b1) * pitch + K);
+                f(std::true_type{}, k, true, __float_as_uint(b0) * pitchS + K);
+                f(std::true_type{}, k + 1, true, __float_as_uint(b1) * pitchS + K);
             }
         } else {
             const uint32_t Ku = Kv - fb.x;
@@ -436,8 +448,8 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
             for (int k = 0; k < LEN; k += 2) {
                 uint32_t bu0, bu1, bv0, bv1;
                 tilted_pair(py[k], py[k + 1], cu, cv, cw, Cu, Cv, Cw, hv, bu0, bu1, bv0, bv1);
-                f(std::true_type{}, k, true, bv0 * pitch + bu0 + Ku);
-                f(std::true_type{}, k + 1, true, bv1 * pitch + bu1 + Ku);
+                f(std::true_type{}, k, true, (bv0 * pitch + bu0 + Ku) * isc + ib);
+                f(std::true_type{}, k + 1, true, (bv1 * pitch + bu1 + Ku) * isc + ib);
             }
         }
         return 2;
@@ -447,7 +459,8 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
         const uint32_t du = fdist(__fmaf_rn(Cu, rw, 0.5f), fb.x);
         const bool in_u = du < fb.y;
         if (!__any_sync(0xffffffffu, in_u)) return 0;
-        const uint32_t K = du + tgt.y;
+        const uint32_t K = (du + tgt.y) * isc + ib;
+        const uint32_t pitchS = pitch * isc;
         const float Qv = __fmul_rn(cv.y, rw), Rv = __fmaf_rn(Cv, rw, hv);
 #pragma unroll
         for (int k = 0; k < LEN; k += 2) {
@@ -455,8 +468,8 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
             fma_rn2(y0, y1, py[k], py[k + 1], Qv, Rv);
             add_rz2(b0, b1, y0, y1, 8388608.0f);
             const uint32_t dv0 = __float_as_uint(b0) - fb.z, dv1 = __float_as_uint(b1) - fb.z;
-            f(std::false_type{}, k, in_u && (dv0 < fb.w), dv0 * pitch + K);
-            f(std::false_type{}, k + 1, in_u && (dv1 < fb.w), dv1 * pitch + K);
+            f(std::false_type{}, k, in_u && (dv0 < fb.w), dv0 * pitchS + K);
+            f(std::false_type{}, k + 1, in_u && (dv1 < fb.w), dv1 * pitchS + K);
         }
     } else {
 #pragma unroll
@@ -464,8 +477,8 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
             uint32_t bu0, bu1, bv0, bv1;
             tilted_pair(py[k], py[k + 1], cu, cv, cw, Cu, Cv, Cw, hv, bu0, bu1, bv0, bv1);
             const uint32_t du0 = bu0 - fb.x, du1 = bu1 - fb.x, dv0 = bv0 - fb.z, dv1 = bv1 - fb.z;
-            f(std::false_type{}, k, (du0 < fb.y) && (dv0 < fb.w), dv0 * pitch + du0 + tgt.y);
-            f(std::false_type{}, k + 1, (du1 < fb.y) && (dv1 < fb.w), dv1 * pitch + du1 + tgt.y);
+            f(std::false_type{}, k, (du0 < fb.y) && (dv0 < fb.w), (dv0 * pitch + du0 + tgt.y) * isc + ib);
+            f(std::false_type{}, k + 1, (du1 < fb.y) && (dv1 < fb.w), (dv1 * pitch + du1 + tgt.y) * isc + ib);
         }
     }
     return 1;
@@ -562,15 +575,17 @@ __device__ __forceinline__ int walk_fast(const ProjMeta &M, const LaunchArgs &a,
 // voxel).
 // CHUNK < LEN walks the column as LEN / CHUNK unrolled chunks in a rolled loop (fewer
 // values live at once); f then sees k whose low bits are compile-time constants.
+// isc / ib as in walk_fast: f receives idx * isc + ib.
 template <int LEN, int CHUNK = LEN, typename F>
 __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a, float nu, float nw, float Pv,
-                                          float Rv, const float *__restrict__ Tk, F &&f)
+                                          float Rv, const float *__restrict__ Tk, F &&f, uint32_t isc = 1u,
+                                          uint32_t ib = 0u)
 {
     static_assert(LEN % 2 == 0 && CHUNK % 4 == 0 && LEN % CHUNK == 0, "columns are walked two voxels at a time");
     const float4 cv = M.cv;
     const int4 rc = M.rect;
     const uint4 tgt = M.tgt;
-    const uint32_t pitch = tgt.x;
+    const uint32_t pitch = tgt.x, pitchS = pitch * isc;
     if (!(M.flags.z & 2)) return -1;  // uniform over the projection
     const float y = __frcp_rn(nw);
     const float ylo = __fmul_rn(__fmaf_rn(-nw, y, 1.0f), y);
@@ -586,7 +601,7 @@ __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a
     };
     if (M.flags.w) {
         // inside: every pixel is in the rectangle, idx = bits * pitch + K (mod 2^32)
-        const uint32_t K = du + tgt.y - base_v * pitch;
+        const uint32_t K = (du + tgt.y - base_v * pitch) * isc + ib;
 #pragma unroll 1
         for (int c0 = 0; c0 < LEN; c0 += CHUNK) {
 #pragma unroll
@@ -594,15 +609,15 @@ __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a
                 const int k = c0 + kk;
                 uint32_t b0, b1;
                 u2unpack(pix_bits2(qv(k >> 1), half, magic), b0, b1);
-                f(std::true_type{}, k, true, b0 * pitch + K);
-                f(std::true_type{}, k + 1, true, b1 * pitch + K);
+                f(std::true_type{}, k, true, b0 * pitchS + K);
+                f(std::true_type{}, k + 1, true, b1 * pitchS + K);
             }
         }
         return 2;
     }
     const bool in_u = (du < (uint32_t)rc.y) && (qu != -0.5f);
     if (!__any_sync(0xffffffffu, in_u)) return 0;
-    const uint32_t K = du + tgt.y;
+    const uint32_t K = (du + tgt.y) * isc + ib;
     const float ex = __fsub_rn(a.row_off_f, 0.5f);  // pix_bits2's one exception
 #pragma unroll 1
     for (int c0 = 0; c0 < LEN; c0 += CHUNK) {
@@ -615,8 +630,8 @@ __device__ __forceinline__ int walk_exact(const ProjMeta &M, const LaunchArgs &a
             u2unpack(pix_bits2(q, half, magic), b0, b1);
             f2unpack(q, q0, q1);
             const uint32_t dv0 = b0 - base_v, dv1 = b1 - base_v;
-            f(std::false_type{}, k, in_u && (dv0 < (uint32_t)rc.w) && (q0 != ex), dv0 * pitch + K);
-            f(std::false_type{}, k + 1, in_u && (dv1 < (uint32_t)rc.w) && (q1 != ex), dv1 * pitch + K);
+            f(std::false_type{}, k, in_u && (dv0 < (uint32_t)rc.w) && (q0 != ex), dv0 * pitchS + K);
+            f(std::false_type{}, k + 1, in_u && (dv1 < (uint32_t)rc.w) && (q1 != ex), dv1 * pitchS + K);
         }
     }
     return 1;
@@ -758,22 +773,36 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
         if constexpr (PYREG) fn(py);
         else fn(s_py2);
     };
-    if (!__syncthreads_or(any)) return;   // an all-zero brick adds nothing
-
+    // the metadata of up to MCAP projections at a time (s_meta holds MCAP entries), one group
+    // of G per warp, all warps at once: the first chunk's before the barrier that tests the
+    // brick.  A group then takes two barriers (tiles complete, tiles flushed).
     const int e_begin = (int)split * (int)a.per_split;
     const int e_end = min((int)a.n_entries, e_begin + (int)a.per_split);
+    auto prepare = [&](int c0, int c1) {
+        for (int w = warp; w * G < c1 - c0; w += NW)
+            compute_meta<ARITH, LIST, false, TCF>(s_meta + w * G, pd, a, c0 + w * G, c1, x0, y0, z0, BX, BYF, BZ,
+                                                  lane);
+    };
+    prepare(e_begin, min(e_end, e_begin + MCAP));
+    if (!__syncthreads_or(any)) return;   // an all-zero brick adds nothing
 
     for (int e0 = e_begin; e0 < e_end; e0 += G) {
-        if (warp == 0) compute_meta<ARITH, LIST, false, TCF>(s_meta, pd, a, e0, e_end, x0, y0, z0, BX, BYF, BZ, lane);
-        __syncthreads();
+        const int buf = (e0 - e_begin) % MCAP;
+        if (buf == 0 && e0 > e_begin) {
+            prepare(e0, min(e_end, e0 + MCAP));
+            __syncthreads();
+        }
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
             // a register copy: the walk's shared-memory atomics would otherwise force the
             // metadata to be re-read from shared memory for every column
-            const ProjMeta M = s_meta[g];
+            const ProjMeta M = s_meta[buf + g];
             const int4 fl = M.flags;
             if (fl.x == kSkip) continue;
             uint32_t *tile = s_tile + g * TCF;
+            // the tile's shared-window address: the tile walks below hand f the atomic's
+            // address (4 * index + tile_s), formed by their one multiply-add per voxel
+            const uint32_t tile_s = (uint32_t)__cvta_generic_to_shared(tile);
             const bool orx = fl.y;
             if constexpr (ARITH == kFast) if (fl.x == kTile) {
                 // FAST into a tile: one lane coordinate is the thread's for all of its columns,
@@ -783,11 +812,11 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 auto splat = [&](const uint4 *vals, float Cu, float Cv, float Cw) {
                     uint4 quad;
                     // a zero adds nothing to a shared-memory tile; no test for it
-                    walk_fast<BYF>(M, a, Cu, Cv, Cw, py, [&](auto, int k, bool in, uint32_t idx) {
+                    walk_fast<BYF>(M, a, Cu, Cv, Cw, py, [&](auto, int k, bool in, uint32_t saddr) {
                         if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
                         const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
-                        if (in) atomicAdd(&tile[idx], v);
-                    });
+                        if (in) red_shared_add(saddr, v);
+                    }, 4u, tile_s);
                 };
                 if (orx) {
                     const float pz = pos<kFast>(a.vmin[2] + z0 + lane, a.voxel[2], a.origin[2]);
@@ -823,11 +852,11 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 auto splat = [&](const uint4 *vals, float nu, float nw, float Pv, float Rv) {
                     uint4 quad;
                     // a zero adds nothing to a shared-memory tile; no test for it
-                    walk_exact<BYF, 8>(M, a, nu, nw, Pv, Rv, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
+                    walk_exact<BYF, 8>(M, a, nu, nw, Pv, Rv, s_meta[buf + g].T, [&](auto, int k, bool in, uint32_t saddr) {
                         if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
                         const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
-                        if (in) atomicAdd(&tile[idx], v);
-                    });
+                        if (in) red_shared_add(saddr, v);
+                    }, 4u, tile_s);
                 };
                 if (orx) {
                     const float pz = pos<kStrict>(a.vmin[2] + z0 + lane, a.voxel[2], a.origin[2]);
@@ -865,7 +894,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                 if (ARITH != kFast && fl.x == kTile) {
                     // a zero adds nothing to a shared-memory tile; no test for it
                     with_py([&](const auto &pyv) {
-                        walk_column<ARITH, BYF, (BYF > 8 ? 8 : BYF)>(M, a, ax, az, pyv, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
+                        walk_column<ARITH, BYF, (BYF > 8 ? 8 : BYF)>(M, a, ax, az, pyv, s_meta[buf + g].T, [&](auto, int k, bool in, uint32_t idx) {
                             if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
                             const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
                             if (in) atomicAdd(&tile[idx], v);
@@ -873,7 +902,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
                     });
                 } else {
                     with_py([&](const auto &pyv) {
-                        walk_column<ARITH, BYF, (BYF > 8 ? 8 : BYF)>(M, a, ax, az, pyv, s_meta[g].T, [&](auto, int k, bool in, uint32_t idx) {
+                        walk_column<ARITH, BYF, (BYF > 8 ? 8 : BYF)>(M, a, ax, az, pyv, s_meta[buf + g].T, [&](auto, int k, bool in, uint32_t idx) {
                             if (!(k & 3)) quad = vals[(k >> 2) * (BZ * VSTRIDE / 4)];
                             const uint32_t v = (k & 2) ? ((k & 1) ? quad.w : quad.z) : ((k & 1) ? quad.y : quad.x);
                             if (in & (v != 0u)) atomicAdd(&sum[idx], v);
@@ -886,7 +915,7 @@ __device__ __forceinline__ void forward_unit(const float *__restrict__ vol, uint
         // flush the tiles: one global atomic per touched pixel, coalesced along rows
 #pragma unroll 1
         for (int g = 0; g < G; ++g) {
-            const ProjMeta &M = s_meta[g];
+            const ProjMeta &M = s_meta[buf + g];
             if (M.flags.x != kTile) continue;
             uint32_t *tile = s_tile + g * TCF;
             const int4 rc = M.rect;
@@ -912,7 +941,7 @@ __global__ void __launch_bounds__(SH::nt, 1024 / SH::nt)
                     const LaunchArgs a, int bricks_x, int bricks_z)
 {
     extern __shared__ uint32_t smem[];
-    __shared__ ProjMeta s_meta[G];
+    __shared__ ProjMeta s_meta[MCAP];
     forward_unit<ARITH, LIST, SH>(vol, sum, pd, a, blockIdx.x, blockIdx.y, bricks_x, bricks_z, smem, s_meta);
 }
 
@@ -1231,6 +1260,30 @@ __global__ void k_preprocess(const float *__restrict__ x, void *out, uint64_t n,
     }
 }
 
+// The preprocessing of k_preprocess applied to images [0, n_img) of W*H pixels in
+// acquisition order, each written to its subset-major slot (j mod S) * Pc + j / S
+// (dataset.hpp:133-140): one launch for a whole request's images.
+template <int ODT>
+__global__ void k_preprocess_reorder(const float *__restrict__ x, void *out, uint64_t wh, uint32_t n_img, uint32_t S,
+                                     uint32_t Pc, int normalize, const float *__restrict__ minmax, int mlog)
+{
+    const float mn = normalize ? minmax[0] : 0.0f, mx = normalize ? minmax[1] : 0.0f;
+    const uint64_t n = wh * n_img;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t j = i / wh, px = i - j * wh;
+        const uint64_t slot = (j % S) * Pc + j / S;
+        float v = x[i];
+        if (normalize) v = is_normal(v) ? __fdiv_rn(__fsub_rn(v, mn), __fsub_rn(mx, mn)) : __fdiv_rn(__fadd_rn(mx, mn), 2.0f);
+        if (mlog) {
+            const float lo = 1.0f - kEps;
+            float c = (lo < v) ? lo : v;          // std::min(v, 1 - eps)
+            c = (c < kEps) ? kEps : c;            // std::max(., eps)
+            v = -p_logf(c);
+        }
+        store_any<ODT>(out, slot * wh + px, v);
+    }
+}
+
 __global__ void k_fill_u32(uint32_t *dst, uint32_t value, uint64_t count)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
@@ -1277,7 +1330,7 @@ __global__ void __launch_bounds__(NT, 4)
     k_forward_batched(const BatchFwdItem *__restrict__ items, int n_items, uint32_t total_units, uint32_t *ticket)
 {
     extern __shared__ uint32_t smem[];
-    __shared__ ProjMeta s_meta[G];
+    __shared__ ProjMeta s_meta[MCAP];
     __shared__ LaunchArgs s_a;
     __shared__ uint32_t s_unit;
     __shared__ int s_item;
@@ -1611,6 +1664,19 @@ cudaError_t launch_preprocess(const float *images, void *out, int odt, uint64_t 
     if (odt == kBF16) k_preprocess<kBF16><<<grid, 256, 0, s>>>(images, out, n, normalize, minmax, mlog);
     else if (odt == kF16) k_preprocess<kF16><<<grid, 256, 0, s>>>(images, out, n, normalize, minmax, mlog);
     else k_preprocess<kF32><<<grid, 256, 0, s>>>(images, out, n, normalize, minmax, mlog);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_preprocess_reorder(const float *images, void *out, int odt, uint64_t wh, uint32_t n_img, uint32_t S,
+                                      uint32_t Pc, int normalize, const float *minmax, int mlog, const DeviceInfo &dev,
+                                      cudaStream_t s)
+{
+    if (wh == 0 || n_img == 0) return cudaSuccess;
+    if (S == 0 || Pc == 0 || n_img > S * Pc) return cudaErrorInvalidValue;
+    const unsigned grid = stream_grid(wh * n_img, dev);
+    if (odt == kBF16) k_preprocess_reorder<kBF16><<<grid, 256, 0, s>>>(images, out, wh, n_img, S, Pc, normalize, minmax, mlog);
+    else if (odt == kF16) k_preprocess_reorder<kF16><<<grid, 256, 0, s>>>(images, out, wh, n_img, S, Pc, normalize, minmax, mlog);
+    else k_preprocess_reorder<kF32><<<grid, 256, 0, s>>>(images, out, wh, n_img, S, Pc, normalize, minmax, mlog);
     return cudaGetLastError();
 }
 
