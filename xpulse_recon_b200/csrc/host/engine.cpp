@@ -361,6 +361,9 @@ struct Engine::Impl {
     {
         return mit == 0 && sit == 0 && p.resume.empty();
     }
+    // the sums' value before the run's first sub-iteration: FIXED(1) where that sub-iteration
+    // skips its forward (reconstruction_n.hpp:60), else zero, as after any sub-iteration
+    static uint32_t first_sums(const Params &p) { return skips_forward(p, p.first_iteration, 0) ? 1u << 22 : 0u; }
 
     void save_layers(const Params &p, const float *vol, int64_t y0, int64_t y1)
     {
@@ -458,7 +461,7 @@ void Engine::reconstruct()
         const std::vector<xpr_projdata> spd = d.subset_projdata();
         check(xpr_upload(d.ctx, pd.p, spd.data(), spd.size() * PDB, d.comp->v()), "upload");
         check(xpr_fill_u32(d.ctx, vol.p, 0x3f800000u, nvol, d.comp->v()), "fill");          // :59
-        check(xpr_fill_u32(d.ctx, sum.p, 1u << 22, Pc * WH, d.comp->v()), "fill");           // :60
+        check(xpr_fill_u32(d.ctx, sum.p, Impl::first_sums(p), Pc * WH, d.comp->v()), "fill");  // :60
         if (!p.resume.empty()) {
             std::vector<float> init(N);
             d.load_layers(p, init.data(), 0, Hv);
@@ -549,7 +552,7 @@ void Engine::reconstruct()
         for (int64_t i = 0; i < (int64_t)N; ++i) hv[i] = init;
         if (!p.resume.empty()) d.load_layers(p, hv, 0, Hv);
         if (!lplh)  // reconstruction_lpla.hpp:243
-            check(xpr_fill_u32(d.ctx, sum.p, 1u << 22, (uint64_t)slots * WH, d.comp->v()), "fill");
+            check(xpr_fill_u32(d.ctx, sum.p, Impl::first_sums(p), (uint64_t)slots * WH, d.comp->v()), "fill");
         double t1 = 0.0;
         if (sync_mode) {
             // method_1a (reconstruction_lpln.hpp:27-96): one slab buffer, every transfer
@@ -785,7 +788,7 @@ void Engine::reconstruct()
             DevBuf img(d.ctx, (uint64_t)Pc * cw * d.iesize), sum(d.ctx, (uint64_t)Pc * cw * 4);
             DevBuf ratio = sep ? DevBuf(d.ctx, (uint64_t)Pc * cw * d.rsize) : DevBuf();
             check(xpr_fill_u32(d.ctx, slab.p, 0x3f800000u, (uint64_t)ny * W * W, d.comp->v()), "fill");
-            check(xpr_fill_u32(d.ctx, sum.p, 1u << 22, (uint64_t)Pc * cw, d.comp->v()), "fill");
+            check(xpr_fill_u32(d.ctx, sum.p, Impl::first_sums(p), (uint64_t)Pc * cw, d.comp->v()), "fill");
             if (!p.resume.empty()) {
                 // the chunk's layers with their padding from the stack (a continuous run's
                 // padding layers are the chunk's own and are not saved, so a resumed chunk

@@ -4,6 +4,7 @@
 #include <string>
 
 #include "../../../include/xpr.h"
+#include "../xpr_internal.h"
 #include "engine.h"
 #include "params.h"
 #include "planner.h"
@@ -71,14 +72,16 @@ int xpr_reconstruct_host(const char *json, const float *images, int64_t count, u
         xpr::Params p = xpr::load_params(json ? json : "{}");
         xpr::Engine eng(p, xpr::memory_images(images, count, width, height), false);
         const uint64_t n = (uint64_t)eng.vwidth() * eng.vheight() * eng.vwidth();
-        if (n > vol_cap) return XPR_ERR_INVALID;
+        if (n > vol_cap)
+            return xpr::set_last_error(XPR_ERR_INVALID, "xpr_reconstruct_host: vol_out holds %llu floats, %llu needed",
+                                       (unsigned long long)vol_cap, (unsigned long long)n);
         eng.set_output(vol_out);  // straight into the caller's buffer
         eng.reconstruct();
         if (seconds) *seconds = eng.stats().seconds_iterations;
         return XPR_OK;
     } catch (const std::exception &e) {
         std::cerr << "xpr_reconstruct_host: " << e.what() << std::endl;
-        return XPR_ERR_PARAM;
+        return xpr::set_last_error(XPR_ERR_PARAM, "xpr_reconstruct_host: %s", e.what());
     }
 }
 
@@ -87,8 +90,8 @@ int xpr_tiff_write(const char *path, const float *data, uint32_t width, uint32_t
     try {
         xpr::tiff_write_f32(path, data, width, height);
         return XPR_OK;
-    } catch (const std::exception &) {
-        return XPR_ERR_IO;
+    } catch (const std::exception &e) {
+        return xpr::set_last_error(XPR_ERR_IO, "xpr_tiff_write: %s", e.what());
     }
 }
 
@@ -100,12 +103,14 @@ int xpr_tiff_read(const char *path, float *data, uint64_t cap, uint32_t *width, 
         if (width) *width = w;
         if (height) *height = h;
         if (data) {
-            if (v.size() > cap) return XPR_ERR_INVALID;
+            if (v.size() > cap)
+                return xpr::set_last_error(XPR_ERR_INVALID, "xpr_tiff_read: the buffer holds %llu floats, %llu needed",
+                                           (unsigned long long)cap, (unsigned long long)v.size());
             std::memcpy(data, v.data(), v.size() * sizeof(float));
         }
         return XPR_OK;
-    } catch (const std::exception &) {
-        return XPR_ERR_IO;
+    } catch (const std::exception &e) {
+        return xpr::set_last_error(XPR_ERR_IO, "xpr_tiff_read: %s", e.what());
     }
 }
 

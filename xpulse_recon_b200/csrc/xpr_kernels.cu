@@ -50,7 +50,7 @@ constexpr int BZ = 32;          // forward brick extent along z
 constexpr int NT = 256;         // threads per CTA (8 warps)
 constexpr int G = 4;            // projections whose tiles are in flight together
 constexpr int TILE_CAP = 1024;  // pixels per shared-memory tile
-constexpr int MCAP = 32;        // forward: projections whose metadata a CTA prepares at once
+constexpr int MCAP = 32;        // projections whose metadata a CTA prepares at once
 static_assert(MCAP % G == 0 && MCAP / G <= NT / 32, "one group of G projections per warp");
 constexpr int VSTRIDE = 132;    // padded row stride (words) of the brick value array: 32 x-positions of four
                                 // layers interleaved, + 4 (128-bit reads bank-conflict free both ways)
@@ -1075,18 +1075,19 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
 #pragma unroll
     for (int k = 0; k < CB / 2; ++k) n2[k] = 0u;
 
-    // metadata double buffer (s_meta holds 2 * G entries): warp 0 prepares the next group
-    // while the CTA walks the current one, so one barrier per group suffices
+    // the metadata of up to MCAP projections at a time (s_meta holds MCAP entries), one group
+    // of G per warp, all warps at once; the walk only reads it, so a chunk takes two barriers
     const int n_entries = (int)a.n_entries;
-    if (warp == 0) compute_meta<ARITH, LIST, true>(s_meta, pd, a, 0, n_entries, x0, y0, z0, BX, CB, BWD_BZ, lane);
-    __syncthreads();
-    for (int e0 = 0, buf = 0; e0 < n_entries; e0 += G, buf ^= G) {
-        if (warp == 0 && e0 + G < n_entries)
-            compute_meta<ARITH, LIST, true>(s_meta + (buf ^ G), pd, a, e0 + G, n_entries, x0, y0, z0, BX, CB, BWD_BZ,
-                                     lane);
+    constexpr int NWB = NT / 32;
+    for (int c0 = 0; c0 < n_entries; c0 += MCAP) {
+        const int c1 = min(n_entries, c0 + MCAP);
+        if (c0 > 0) __syncthreads();  // the previous chunk's metadata read by every warp
+        for (int w = warp; w * G < c1 - c0; w += NWB)
+            compute_meta<ARITH, LIST, true>(s_meta + w * G, pd, a, c0 + w * G, c1, x0, y0, z0, BX, CB, BWD_BZ, lane);
+        __syncthreads();
 #pragma unroll 1
-        for (int g = 0; g < G; ++g) {
-            const ProjMeta &M = s_meta[buf + g];
+        for (int e = 0; e < c1 - c0; ++e) {
+            const ProjMeta &M = s_meta[e];
             if (M.flags.x == kSkip) continue;
             // the column's gathers are issued before any is consumed (all in flight together);
             // an out-of-bounds pair contributes r = 0, and s + 0 == s exactly (s is never -0).
@@ -1122,7 +1123,6 @@ __device__ __forceinline__ void backward_unit(float *__restrict__ vol, const voi
             if (!NANSKIP && walked == 2) ++n_inside;
             consume(CB / 2);
         }
-        __syncthreads();
     }
     const int sx = a.size[0], sy = a.size[1], sz = a.size[2];
     const int x = x0 + lane, z = z0 + warp;
@@ -1144,7 +1144,7 @@ __global__ void __launch_bounds__(NT, 4)
     k_backward_tiled(float *__restrict__ vol, const void *__restrict__ ratio, const xpr_projdata *__restrict__ pd,
                      const LaunchArgs a, int bricks_x, int bricks_z)
 {
-    __shared__ ProjMeta s_meta[2 * G];
+    __shared__ ProjMeta s_meta[MCAP];
     backward_unit<ARITH, LIST, NANSKIP, DT, CB>(vol, ratio, pd, a, blockIdx.x, bricks_x, bricks_z, s_meta);
 }
 
@@ -1361,7 +1361,7 @@ template <int ARITH, int DT, int CB>
 __global__ void __launch_bounds__(NT, 4)
     k_backward_batched(const BatchBwdItem *__restrict__ items, int n_items, uint32_t total_units, uint32_t *ticket)
 {
-    __shared__ ProjMeta s_meta[2 * G];
+    __shared__ ProjMeta s_meta[MCAP];
     __shared__ LaunchArgs s_a;
     __shared__ uint32_t s_unit;
     __shared__ int s_item;
