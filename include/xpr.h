@@ -207,6 +207,8 @@ typedef struct xpr_batch_opts {
     int32_t ctas_per_sm;          /* 0: the occupancy limit */
     int32_t image_storage_set;    /* 0: the measured images are stored in `storage` too */
     int32_t image_storage;        /* else their xpr_dtype, e.g. FP16 images with a BF16 ratio */
+    int32_t fwd_layers;           /* 0: automatic or tuned; else the forward brick's layers: 8, or 16
+                                     in the STRICT contract */
 } xpr_batch_opts;
 
 typedef struct xpr_batch xpr_batch;
@@ -220,10 +222,11 @@ int xpr_batch_run(xpr_batch *b, void *stream);
 /* One step: sub-iteration `step` of every problem that has one (step < xpr_batch_steps). */
 int xpr_batch_step(xpr_batch *b, uint32_t step, void *stream);
 uint32_t xpr_batch_steps(const xpr_batch *b);
-/* The schedule in use: projection runs per forward brick, backward column length,
- * persistent CTAs per SM, and the tuned step time in ms (0 when not tuned). */
-int xpr_batch_schedule(const xpr_batch *b, int32_t *fwd_splits, int32_t *bwd_column, int32_t *ctas_per_sm,
-                       double *tuned_ms);
+/* The schedule in use: projection runs per forward brick, the forward brick's layers,
+ * backward column length, persistent forward CTAs per SM, and the tuned step time in ms
+ * (0 when not tuned). */
+int xpr_batch_schedule(const xpr_batch *b, int32_t *fwd_splits, int32_t *fwd_layers, int32_t *bwd_column,
+                       int32_t *ctas_per_sm, double *tuned_ms);
 int xpr_batch_destroy(xpr_batch *b);
 
 /* ---------------------------------------------------------------- serving */

@@ -72,13 +72,15 @@ def test_batch_equals_each_problem_alone(bctx, storage):
     b.close()
 
 
-@pytest.mark.parametrize("splits,column", [(1, 16), (3, 8), (8, 16)])
-def test_schedule_does_not_change_results(bctx, splits, column):
+@pytest.mark.parametrize("splits,layers,column", [(1, 16, 16), (3, 8, 8), (8, 16, 16), (2, 8, 16)])
+def test_schedule_does_not_change_results(bctx, splits, layers, column):
     probs = _problems(bctx, _lib.F32)
     alone = _alone(bctx, probs, _lib.STRICT, _lib.F32)
-    b = Batch(bctx, probs, use_graph=False, autotune=False, fwd_splits=splits, bwd_column=column, ctas_per_sm=2)
+    b = Batch(bctx, probs, use_graph=False, autotune=False, fwd_splits=splits, bwd_column=column, ctas_per_sm=2,
+              fwd_layers=layers)
     sch = b.schedule()
     assert sch["fwd_splits"] == splits and sch["bwd_column"] == column and sch["ctas_per_sm"] <= 2
+    assert sch["fwd_layers"] == layers
     for p in probs:  # xpr_batch_step does not initialise the volumes; xpr_batch_run does
         p.vol.fill_(1.0)
     for k in range(b.steps):  # step by step, as a serving loop drives it
@@ -128,3 +130,11 @@ def test_bad_problem_is_rejected(bctx):
     probs[0].sit = 0
     with pytest.raises(_lib.XprError, match="sit"):
         Batch(bctx, probs)
+
+
+def test_sixteen_layer_forward_is_strict_only(bctx):
+    probs = _problems(bctx, _lib.F32)[:1]
+    with pytest.raises(_lib.XprError, match="fwd_layers"):
+        Batch(bctx, probs, arith=_lib.FAST, fwd_layers=16)
+    with pytest.raises(_lib.XprError, match="fwd_layers"):
+        Batch(bctx, probs, arith=_lib.STRICT, fwd_layers=12)

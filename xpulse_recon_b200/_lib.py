@@ -69,7 +69,7 @@ class BatchOpts(C.Structure):
     _fields_ = [("arith", C.c_int32), ("storage", C.c_int32), ("init_volume", C.c_int32),
                 ("use_graph", C.c_int32), ("autotune", C.c_int32), ("fwd_splits", C.c_int32),
                 ("bwd_column", C.c_int32), ("ctas_per_sm", C.c_int32), ("image_storage_set", C.c_int32),
-                ("image_storage", C.c_int32)]
+                ("image_storage", C.c_int32), ("fwd_layers", C.c_int32)]
 
 
 _lib = None
@@ -121,7 +121,7 @@ def lib():
     _sig(L, "xpr_batch_step", i32, [vp, C.c_uint32, vp])
     _sig(L, "xpr_batch_steps", C.c_uint32, [vp])
     _sig(L, "xpr_batch_schedule", i32, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
-                                        C.POINTER(C.c_double)])
+                                        C.POINTER(C.c_int32), C.POINTER(C.c_double)])
     _sig(L, "xpr_batch_destroy", i32, [vp])
     _lib = L
     return L

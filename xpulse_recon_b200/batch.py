@@ -122,13 +122,14 @@ class Batch:
 
     def __init__(self, ctx: Context, problems: list, arith: int = _lib.STRICT, storage: int = _lib.F32,
                  init_volume: bool = True, use_graph: bool = True, autotune: bool = True, fwd_splits: int = 0,
-                 bwd_column: int = 0, ctas_per_sm: int = 0, image_storage: int = None):
-        """storage: the ratio's dtype, and the images' unless image_storage is given."""
+                 bwd_column: int = 0, ctas_per_sm: int = 0, image_storage: int = None, fwd_layers: int = 0):
+        """storage: the ratio's dtype, and the images' unless image_storage is given;
+        fwd_layers: the forward brick's layers (0: automatic or tuned; 8, or 16 in STRICT)."""
         self.ctx, self.problems = ctx, list(problems)
         arr = (_lib.BatchProblem * len(self.problems))(*[p.c_struct() for p in self.problems])
         o = _lib.BatchOpts(arith, storage, int(init_volume), int(use_graph), int(autotune), fwd_splits, bwd_column,
                            ctas_per_sm, int(image_storage is not None),
-                           storage if image_storage is None else image_storage)
+                           storage if image_storage is None else image_storage, fwd_layers)
         h = C.c_void_p()
         check(lib().xpr_batch_create(ctx.handle, arr, len(self.problems), C.byref(o), _stream(), C.byref(h)),
               "xpr_batch_create")
@@ -145,10 +146,11 @@ class Batch:
         check(lib().xpr_batch_step(self.handle, k, _stream() if stream is None else stream), "xpr_batch_step")
 
     def schedule(self) -> dict:
-        s, c, n, t = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
-        check(lib().xpr_batch_schedule(self.handle, C.byref(s), C.byref(c), C.byref(n), C.byref(t)),
+        s, ly, c, n, t = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        check(lib().xpr_batch_schedule(self.handle, C.byref(s), C.byref(ly), C.byref(c), C.byref(n), C.byref(t)),
               "xpr_batch_schedule")
-        return {"fwd_splits": s.value, "bwd_column": c.value, "ctas_per_sm": n.value, "tuned_ms": t.value}
+        return {"fwd_splits": s.value, "fwd_layers": ly.value, "bwd_column": c.value, "ctas_per_sm": n.value,
+                "tuned_ms": t.value}
 
     def close(self) -> None:
         if self.handle:

@@ -37,7 +37,7 @@ struct StepPlan {
 // tuned schedules, per batch shape
 using ShapeKey = std::tuple<int, int, int, std::vector<uint64_t>>;
 std::mutex g_tune_mu;
-std::map<ShapeKey, std::tuple<int, int, double>> g_tuned;
+std::map<ShapeKey, std::tuple<int, int, int, double>> g_tuned;  // splits, layers, column, step ms
 
 }  // namespace
 
@@ -54,7 +54,7 @@ struct xpr_batch {
     xpr::BatchFillItem *fills = nullptr;   // [0, n): volumes <- 1.0, [n, 2n): sums <- 0, [2n, 3n): ratios <- 0
     uint64_t max_vol = 0, max_pix = 0, max_ratio_words = 0;
     std::vector<StepPlan> plan;
-    int splits = 1, column = 16, ctas = 0;
+    int splits = 1, layers = 8, column = 16, ctas = 0;
     unsigned grid_fwd = 0, grid_bwd = 0;   // persistent CTAs of the forward / backward launches
     double tuned_ms = 0.0;
     cudaStream_t capture = nullptr;
@@ -74,12 +74,12 @@ int cuda_fail(cudaError_t e, const char *what)
 // (or the requested number below it) on every SM
 unsigned grid_of(const xpr_batch *b, int kind)
 {
-    const int occ = xpr::batched_ctas_per_sm(kind, b->opts.arith, b->opts.storage, b->column);
+    const int occ = xpr::batched_ctas_per_sm(kind, b->opts.arith, b->opts.storage, kind == 0 ? b->layers : b->column);
     const int per_sm = b->ctas > 0 ? std::min(b->ctas, std::max(occ, 1)) : std::max(occ, 1);
     return (unsigned)(b->di->sm_count * per_sm);
 }
 
-int build_lists(xpr_batch *b, int splits, int column, cudaStream_t s)
+int build_lists(xpr_batch *b, int splits, int layers, int column, cudaStream_t s)
 {
     std::vector<char> host;
     b->plan.assign(b->steps, StepPlan{});
@@ -94,7 +94,7 @@ int build_lists(xpr_batch *b, int splits, int column, cudaStream_t s)
         StepPlan &P = b->plan[k];
         it.clear();
         for (const auto &pp : b->probs)
-            if (k < pp.steps() && !xpr::add_step_items(pp, k, splits, column, b->opts.image_storage, &it))
+            if (k < pp.steps() && !xpr::add_step_items(pp, k, splits, layers, column, b->opts.image_storage, &it))
                 return fail(XPR_ERR_UNSUPPORTED, "batch step exceeds 2^31 work units");
         P.n_fwd = (int)it.fwd.size();
         P.n_err = (int)it.err.size();
@@ -120,6 +120,7 @@ int build_lists(xpr_batch *b, int splits, int column, cudaStream_t s)
         if (e2 != cudaSuccess) return cuda_fail(e2, "work-list upload");
     }
     b->splits = splits;
+    b->layers = layers;
     b->column = column;
     b->grid_fwd = grid_of(b, 0);
     b->grid_bwd = grid_of(b, 1);
@@ -141,7 +142,7 @@ cudaError_t enqueue_forward(xpr_batch *b, uint32_t k, cudaStream_t s)
     const StepPlan &P = b->plan[k];
     if (!P.n_fwd) return cudaSuccess;
     return xpr::launch_forward_batched((const xpr::BatchFwdItem *)((char *)b->lists + P.fwd_off), P.n_fwd,
-                                       P.fwd_units, b->tickets, b->opts.arith, b->grid_fwd, s);
+                                       P.fwd_units, b->tickets, b->opts.arith, b->layers, b->grid_fwd, s);
 }
 
 cudaError_t enqueue_backward(xpr_batch *b, uint32_t k, cudaStream_t s)
@@ -199,8 +200,8 @@ float time_ms(cudaStream_t s, F &&fn)
 }
 
 // Candidate schedules, timed on the batch's own data: the forward of step 1 (sums are
-// cleared after) for each projection-run split, the backward of step 0 against zero
-// ratios for each column length.  exp(0 / count) is exactly 1, so a voxel is unchanged
+// cleared after) for each forward brick (8 layers, and 16 in the STRICT contract) and
+// projection-run split, the backward of step 0 against zero ratios for each column length.  exp(0 / count) is exactly 1, so a voxel is unchanged
 // unless no projection of step 0 reaches it (count 0), and those voxels become NaN in
 // step 0 of the run as well.
 int autotune(xpr_batch *b, cudaStream_t s)
@@ -217,33 +218,37 @@ int autotune(xpr_batch *b, cudaStream_t s)
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tuned.find(key);
         if (it != g_tuned.end()) {
-            b->tuned_ms = std::get<2>(it->second);
-            return build_lists(b, std::get<0>(it->second), std::get<1>(it->second), s);
+            b->tuned_ms = std::get<3>(it->second);
+            return build_lists(b, std::get<0>(it->second), std::get<1>(it->second), std::get<2>(it->second), s);
         }
     }
-    int best_s = b->splits, best_c = b->column;
+    int best_s = b->splits, best_l = b->layers, best_c = b->column;
     float best_f = 0.0f, best_b = 0.0f;
     if (b->steps > 1) {
         bool first = true;
-        for (int sp : {1, 2, 4, 8, 16}) {
-            if (sp > 1 && (uint32_t)sp > xpr::div_up(max_e, 4)) break;
-            if (int rc = build_lists(b, sp, b->column, s)) return rc;
-            const float ms = time_ms(s, [&] {
-                enqueue_forward(b, 1, s);
-                enqueue_fill(b, 1, s);
-            });
-            if (first || ms < best_f) {
-                best_f = ms;
-                best_s = sp;
+        for (int ly : {8, 16}) {
+            if (!xpr::forward_layers_ok(b->opts.arith, ly)) continue;
+            for (int sp : {1, 2, 4, 8, 16}) {
+                if (sp > 1 && (uint32_t)sp > xpr::div_up(max_e, 4)) break;
+                if (int rc = build_lists(b, sp, ly, b->column, s)) return rc;
+                const float ms = time_ms(s, [&] {
+                    enqueue_forward(b, 1, s);
+                    enqueue_fill(b, 1, s);
+                });
+                if (first || ms < best_f) {
+                    best_f = ms;
+                    best_s = sp;
+                    best_l = ly;
+                }
+                first = false;
             }
-            first = false;
         }
     }
     cudaError_t e = enqueue_fill(b, 2, s);
     if (e != cudaSuccess) return cuda_fail(e, "autotune");
     bool first = true;
     for (int cb : {16, 8}) {
-        if (int rc = build_lists(b, best_s, cb, s)) return rc;
+        if (int rc = build_lists(b, best_s, best_l, cb, s)) return rc;
         const float ms = time_ms(s, [&] { enqueue_backward(b, 0, s); });
         if (first || ms < best_b) {
             best_b = ms;
@@ -256,9 +261,9 @@ int autotune(xpr_batch *b, cudaStream_t s)
     b->tuned_ms = (double)best_f + (double)best_b;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tuned[key] = std::make_tuple(best_s, best_c, b->tuned_ms);
+        g_tuned[key] = std::make_tuple(best_s, best_l, best_c, b->tuned_ms);
     }
-    return build_lists(b, best_s, best_c, s);
+    return build_lists(b, best_s, best_l, best_c, s);
 }
 
 void release(xpr_batch *b)
@@ -294,6 +299,8 @@ int xpr_batch_create(xpr_ctx *ctx, const xpr_batch_problem *problems, uint32_t n
         return fail(XPR_ERR_INVALID, "unknown image storage dtype");
     if (o.bwd_column != 0 && o.bwd_column != 8 && o.bwd_column != 16)
         return fail(XPR_ERR_INVALID, "bwd_column must be 0, 8 or 16");
+    if (o.fwd_layers != 0 && !xpr::forward_layers_ok(o.arith, o.fwd_layers))
+        return fail(XPR_ERR_INVALID, "fwd_layers must be 0 or 8 (FAST), 0, 8 or 16 (STRICT)");
     cudaError_t e = xpr::prepare_device_kernels();
     if (e != cudaSuccess) return cuda_fail(e, "xpr_batch_create");
 
@@ -304,6 +311,7 @@ int xpr_batch_create(xpr_ctx *ctx, const xpr_batch_problem *problems, uint32_t n
     b->ctas = o.ctas_per_sm;
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     uint64_t scratch_bytes = 0;
+    const int layers = o.fwd_layers ? o.fwd_layers : (o.arith == XPR_ARITH_STRICT ? 16 : 8);
     uint64_t total_bricks = 0;
     uint32_t max_e = 0;
     b->probs.resize(n);
@@ -319,7 +327,9 @@ int xpr_batch_create(xpr_ctx *ctx, const xpr_batch_problem *problems, uint32_t n
         b->max_vol = std::max<uint64_t>(b->max_vol, (uint64_t)p.vwidth * p.vheight * p.vwidth);
         b->max_pix = std::max(b->max_pix, npix);
         b->max_ratio_words = std::max<uint64_t>(b->max_ratio_words, xpr::div_up(npix * xpr::dtype_size(o.storage), 4));
-        total_bricks += xpr::div_up(p.vwidth, 32) * xpr::div_up(p.vwidth, 32) * xpr::div_up(p.vheight, 8);
+        total_bricks += xpr::div_up(p.vwidth, xpr::forward_brick(0, layers)) *
+                        xpr::div_up(p.vwidth, xpr::forward_brick(2, layers)) *
+                        xpr::div_up(p.vheight, xpr::forward_brick(1, layers));
         max_e = std::max(max_e, xpr::entries_of(p));
     }
     scratch_bytes += 256 + 3 * sizeof(xpr::BatchFillItem) * n;
@@ -352,22 +362,24 @@ int xpr_batch_create(xpr_ctx *ctx, const xpr_batch_problem *problems, uint32_t n
         release(b);
         return cuda_fail(e, "xpr_batch_create");
     }
-    // default schedule: split projection runs only when the batch has too few bricks to
-    // fill the GPU (3 waves of the forward's 4 CTAs per SM)
+    // default schedule: 16-layer forward bricks in the STRICT contract (its per-column work
+    // spread over more voxels), 8 in FAST; split projection runs only when the batch has too
+    // few bricks to fill the GPU (3 waves of the forward's resident CTAs)
     int splits = o.fwd_splits;
     if (splits <= 0) {
-        const uint64_t target = (uint64_t)di->sm_count * 4 * 3;
+        const uint64_t target = (uint64_t)di->sm_count *
+                                std::max(1, xpr::batched_ctas_per_sm(0, o.arith, o.storage, layers)) * 3;
         splits = total_bricks >= target
                      ? 1
                      : (int)std::min<uint64_t>(xpr::div_up(target, total_bricks), xpr::div_up(max_e, 4));
         splits = std::max(splits, 1);
     }
     const int column = o.bwd_column ? o.bwd_column : 16;
-    if (int rc = build_lists(b, splits, column, s)) {
+    if (int rc = build_lists(b, splits, layers, column, s)) {
         release(b);
         return rc;
     }
-    if (o.autotune && o.fwd_splits <= 0 && o.bwd_column == 0) {
+    if (o.autotune && o.fwd_splits <= 0 && o.fwd_layers == 0 && o.bwd_column == 0) {
         if (int rc = autotune(b, s)) {
             release(b);
             return rc;
@@ -420,11 +432,12 @@ int xpr_batch_run(xpr_batch *b, void *stream)
     return e == cudaSuccess ? XPR_OK : cuda_fail(e, "xpr_batch_run: graph launch");
 }
 
-int xpr_batch_schedule(const xpr_batch *b, int32_t *fwd_splits, int32_t *bwd_column, int32_t *ctas_per_sm,
-                       double *tuned_ms)
+int xpr_batch_schedule(const xpr_batch *b, int32_t *fwd_splits, int32_t *fwd_layers, int32_t *bwd_column,
+                       int32_t *ctas_per_sm, double *tuned_ms)
 {
     if (!b) return fail(XPR_ERR_INVALID, "xpr_batch_schedule: NULL batch");
     if (fwd_splits) *fwd_splits = b->splits;
+    if (fwd_layers) *fwd_layers = b->layers;
     if (bwd_column) *bwd_column = b->column;
     if (ctas_per_sm) *ctas_per_sm = (int32_t)(b->grid_fwd / (unsigned)b->di->sm_count);
     if (tuned_ms) *tuned_ms = b->tuned_ms;

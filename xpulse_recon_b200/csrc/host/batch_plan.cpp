@@ -39,7 +39,8 @@ const char *plan_problem(const xpr_batch_problem &p, int arith, PlannedProblem *
     return nullptr;
 }
 
-bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int column, int image_dtype, StepItems *out)
+bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int layers, int column, int image_dtype,
+                    StepItems *out)
 {
     const xpr_batch_problem &p = pp.p;
     const uint32_t s_idx = k % p.sit;
@@ -55,11 +56,11 @@ bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int column
         f.vol = p.vol;
         f.sum = pp.sums;
         f.pd = pd;
-        f.bricks_x = (int)div_up(p.vwidth, forward_brick(0));
-        f.bricks_z = (int)div_up(p.vwidth, forward_brick(2));
+        f.bricks_x = (int)div_up(p.vwidth, forward_brick(0, layers));
+        f.bricks_z = (int)div_up(p.vwidth, forward_brick(2, layers));
         f.splits = (uint32_t)div_up(E, f.a.per_split);
         f.unit_begin = out->fwd_units;
-        const uint64_t units = (uint64_t)f.bricks_x * f.bricks_z * div_up(p.vheight, forward_brick(1)) * f.splits;
+        const uint64_t units = (uint64_t)f.bricks_x * f.bricks_z * div_up(p.vheight, forward_brick(1, layers)) * f.splits;
         if (out->fwd_units + units >= (1ull << 31)) return false;
         out->fwd_units += (uint32_t)units;
         out->fwd.push_back(f);

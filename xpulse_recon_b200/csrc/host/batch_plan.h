@@ -15,10 +15,12 @@ namespace xpr {
 inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 inline size_t dtype_size(int dt) { return dt == XPR_F32 ? 4 : 2; }
 inline uint32_t entries_of(const xpr_batch_problem &p) { return p.per_subset * (p.modules ? p.modules : 1u); }
-// entries per forward work unit (a multiple of the metadata group of 4) for `splits` runs
+// entries per forward work unit for `splits` runs of equal length (a run need not be a
+// whole number of metadata groups: the last group of a run marks its missing entries
+// skipped)
 inline uint32_t per_split_for(uint32_t entries, int splits)
 {
-    return (uint32_t)div_up(div_up(entries, (uint64_t)(splits > 1 ? splits : 1)), 4) * 4;
+    return (uint32_t)div_up(entries, (uint64_t)(splits > 1 ? splits : 1));
 }
 
 struct PlannedProblem {
@@ -53,7 +55,9 @@ struct StepItems {
 };
 
 // Appends sub-iteration k of `pp` (k < pp.steps()); false when the step would exceed 2^31
-// work units.  splits: projection runs per forward brick; column: backward column length.
-bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int column, int image_dtype, StepItems *out);
+// work units.  splits: projection runs per forward brick; layers: the forward brick's
+// layers (8, or 16 in the STRICT contract); column: backward column length.
+bool add_step_items(const PlannedProblem &pp, uint32_t k, int splits, int layers, int column, int image_dtype,
+                    StepItems *out);
 
 }  // namespace xpr

@@ -106,6 +106,7 @@ struct xpr_server {
     size_t items_cap = 0;
     cudaEvent_t tick_ev[2] = {nullptr, nullptr};
     unsigned grid_fwd = 0, grid_bwd = 0;
+    int layers = 8;  // forward brick layers
     std::thread io_thread, compute_thread, dl_thread;
 };
 
@@ -428,15 +429,17 @@ void compute_loop(xpr_server *s)
         uint64_t bricks = 0, max_e = 0, pairs = 0;
         for (Request *r : act) {
             const auto &p = r->pp.p;
-            bricks += xpr::div_up(p.vwidth, 32) * xpr::div_up(p.vwidth, 32) * xpr::div_up(p.vheight, 8);
+            bricks += xpr::div_up(p.vwidth, xpr::forward_brick(0, s->layers)) *
+                      xpr::div_up(p.vwidth, xpr::forward_brick(2, s->layers)) *
+                      xpr::div_up(p.vheight, xpr::forward_brick(1, s->layers));
             max_e = std::max<uint64_t>(max_e, xpr::entries_of(p));
         }
-        const uint64_t target = (uint64_t)s->di->sm_count * 4 * 3;
+        const uint64_t target = (uint64_t)s->grid_fwd * 3;  // three waves of the forward's resident CTAs
         const int splits = bricks >= target ? 1 : (int)std::max<uint64_t>(
                                                         1, std::min(xpr::div_up(target, bricks), xpr::div_up(max_e, 4)));
         bool ok = true;
         for (Request *r : act) {
-            ok = ok && xpr::add_step_items(r->pp, r->step, splits, 16, s->opts.image_storage, &items);
+            ok = ok && xpr::add_step_items(r->pp, r->step, splits, s->layers, 16, s->opts.image_storage, &items);
             pairs += r->N * (uint64_t)r->Pc;
         }
         const size_t fb = items.fwd.size() * sizeof(items.fwd[0]), eb = items.err.size() * sizeof(items.err[0]),
@@ -468,7 +471,7 @@ void compute_loop(xpr_server *s)
             if (e == cudaSuccess) e = cudaEventRecord(s->tick_ev[h], s->comp);
             if (e == cudaSuccess && !items.fwd.empty())
                 e = xpr::launch_forward_batched((const xpr::BatchFwdItem *)db, (int)items.fwd.size(), items.fwd_units,
-                                                s->tickets, s->opts.arith, s->grid_fwd, s->comp);
+                                                s->tickets, s->opts.arith, s->layers, s->grid_fwd, s->comp);
             if (e == cudaSuccess)
                 e = xpr::launch_error_batched((const xpr::BatchErrItem *)(db + eo), (int)items.err.size(),
                                               s->opts.image_storage, s->opts.storage, items.max_n, *s->di, s->comp);
@@ -628,7 +631,9 @@ int xpr_serve_create(xpr_ctx *ctx, const xpr_serve_opts *opts, xpr_server **out)
         release(s);
         return fail(XPR_ERR_CUDA, "xpr_serve_create: streams / staging");
     }
-    s->grid_fwd = (unsigned)(di->sm_count * std::max(1, xpr::batched_ctas_per_sm(0, o.arith, o.storage, 16)));
+    // 16-layer forward bricks in the STRICT contract (its per-column work spread over more voxels)
+    s->layers = o.arith == XPR_ARITH_STRICT ? 16 : 8;
+    s->grid_fwd = (unsigned)(di->sm_count * std::max(1, xpr::batched_ctas_per_sm(0, o.arith, o.storage, s->layers)));
     s->grid_bwd = (unsigned)(di->sm_count * std::max(1, xpr::batched_ctas_per_sm(1, o.arith, o.storage, 16)));
     s->io_thread = std::thread(io_loop, s);
     s->compute_thread = std::thread(compute_loop, s);

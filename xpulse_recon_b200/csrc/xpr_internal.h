@@ -114,11 +114,13 @@ struct BatchFillItem {
 };
 
 // forward brick / backward brick extents (work-unit geometry for the host planner)
-int forward_brick(int axis);               // 0: x, 1: y, 2: z
+int forward_brick(int axis, int layers);   // 0: x, 1: y (the brick's layers: 8, or 16 in STRICT), 2: z
+bool forward_layers_ok(int arith, int layers);
 int backward_brick(int axis, int cb);
-int batched_ctas_per_sm(int kind, int arith, int dtype, int cb);  // kind 0: forward, 1: backward
+// kind 0: forward (cb = its brick layers), 1: backward (cb = its column length)
+int batched_ctas_per_sm(int kind, int arith, int dtype, int cb);
 cudaError_t launch_forward_batched(const BatchFwdItem *items, int n_items, uint32_t total_units, uint32_t *ticket,
-                                   int arith, unsigned ctas, cudaStream_t s);
+                                   int arith, int layers, unsigned ctas, cudaStream_t s);
 cudaError_t launch_backward_batched(const BatchBwdItem *items, int n_items, uint32_t total_units, uint32_t *ticket,
                                     int arith, int dtype, int cb, unsigned ctas, cudaStream_t s);
 cudaError_t launch_error_batched(const BatchErrItem *items, int n_items, int image_dtype, int ratio_dtype,

@@ -1325,8 +1325,8 @@ __device__ __forceinline__ void ticket_depart(uint32_t *ticket)
     }
 }
 
-template <int ARITH>
-__global__ void __launch_bounds__(NT, 4)
+template <int ARITH, typename SH = FwdNarrow>
+__global__ void __launch_bounds__(SH::nt, 1024 / SH::nt)
     k_forward_batched(const BatchFwdItem *__restrict__ items, int n_items, uint32_t total_units, uint32_t *ticket)
 {
     extern __shared__ uint32_t smem[];
@@ -1350,8 +1350,8 @@ __global__ void __launch_bounds__(NT, 4)
         if (u >= total_units) break;
         const BatchFwdItem &I = items[s_item];
         const uint32_t local = u - I.unit_begin, splits = I.splits;
-        forward_unit<ARITH, false>(I.vol, I.sum, I.pd, s_a, local / splits, local % splits, I.bricks_x, I.bricks_z,
-                                   smem, s_meta);
+        forward_unit<ARITH, false, SH>(I.vol, I.sum, I.pd, s_a, local / splits, local % splits, I.bricks_x,
+                                       I.bricks_z, smem, s_meta);
         __syncthreads();
     }
     ticket_depart(ticket);
@@ -1488,10 +1488,12 @@ cudaError_t prepare_device_kernels()
         e = cudaFuncSetAttribute(f.f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem);
         if (e != cudaSuccess) return e;
     }
-    void (*bfns[])(const BatchFwdItem *, int, uint32_t, uint32_t *) = {k_forward_batched<kStrict>,
-                                                                       k_forward_batched<kFast>};
-    for (auto f : bfns) {
-        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    using BFwdFn = void (*)(const BatchFwdItem *, int, uint32_t, uint32_t *);
+    const struct { BFwdFn f; size_t smem; } bfns[] = {{k_forward_batched<kStrict>, (size_t)smem},
+                                                      {k_forward_batched<kFast>, (size_t)smem},
+                                                      {k_forward_batched<kStrict, FwdTall>, FwdTall::smem}};
+    for (const auto &f : bfns) {
+        e = cudaFuncSetAttribute(f.f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem);
         if (e != cudaSuccess) return e;
     }
     if (dev < 64) g_attr_done[dev] = true;
@@ -1513,7 +1515,10 @@ static cudaError_t forward_tiled(const float *vol, uint32_t *sum, const xpr_proj
         splits = (uint32_t)std::min<uint64_t>((target + bricks - 1) / bricks, (a.n_entries + G - 1) / G);
         splits = std::max<uint32_t>(splits, 1);
     }
-    a.per_split = (((a.n_entries + splits - 1) / splits) + G - 1) / G * G;
+    // runs of equal length (a run need not be a whole number of metadata groups: the last
+    // group of a run marks its missing entries skipped), so no CTA of the grid holds a short
+    // remainder while the others walk full runs
+    a.per_split = (a.n_entries + splits - 1) / splits;
     splits = (a.n_entries + a.per_split - 1) / std::max<uint32_t>(a.per_split, 1);
     if (splits == 0) splits = 1;
     if (a.n_entries > 0 && bricks > 0) {
@@ -1699,7 +1704,8 @@ cudaError_t launch_convert(const float *src, void *dst, int dtype, uint64_t n, c
 }
 
 // ---- batched launchers ---------------------------------------------------------------
-int forward_brick(int axis) { return axis == 0 ? BX : (axis == 1 ? BY : BZ); }
+int forward_brick(int axis, int layers) { return axis == 0 ? BX : (axis == 1 ? layers : BZ); }
+bool forward_layers_ok(int arith, int layers) { return layers == BY || (layers == FwdTall::by && arith == kStrict); }
 int backward_brick(int axis, int cb) { return axis == 0 ? BX : (axis == 1 ? cb : BWD_BZ); }
 
 template <int AR, int DT>
@@ -1708,9 +1714,14 @@ static void *bwd_batched_fn(int cb)
     return cb == 8 ? (void *)k_backward_batched<AR, DT, 8> : (void *)k_backward_batched<AR, DT, 16>;
 }
 
+// kind 0: the forward, cb its brick layers (8, or 16 in the STRICT contract); kind 1: the
+// backward, cb its column length
 static void *batched_fn(int kind, int arith, int dtype, int cb)
 {
-    if (kind == 0) return arith == kFast ? (void *)k_forward_batched<kFast> : (void *)k_forward_batched<kStrict>;
+    if (kind == 0) {
+        if (arith == kFast) return (void *)k_forward_batched<kFast>;
+        return cb == FwdTall::by ? (void *)k_forward_batched<kStrict, FwdTall> : (void *)k_forward_batched<kStrict>;
+    }
     if (arith == kFast) {
         if (dtype == kBF16) return bwd_batched_fn<kFast, kBF16>(cb);
         if (dtype == kF16) return bwd_batched_fn<kFast, kF16>(cb);
@@ -1725,8 +1736,10 @@ int batched_ctas_per_sm(int kind, int arith, int dtype, int cb)
 {
     if (prepare_device_kernels() != cudaSuccess) return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batched_fn(kind, arith, dtype, cb), NT,
-                                                      kind == 0 ? kFwdSmem : 0) != cudaSuccess) {
+    const bool tall = kind == 0 && arith == kStrict && cb == FwdTall::by;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batched_fn(kind, arith, dtype, cb), tall ? FwdTall::nt : NT,
+                                                      kind == 0 ? (tall ? FwdTall::smem : kFwdSmem) : 0) !=
+        cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -1734,13 +1747,17 @@ int batched_ctas_per_sm(int kind, int arith, int dtype, int cb)
 }
 
 cudaError_t launch_forward_batched(const BatchFwdItem *items, int n_items, uint32_t total_units, uint32_t *ticket,
-                                   int arith, unsigned ctas, cudaStream_t s)
+                                   int arith, int layers, unsigned ctas, cudaStream_t s)
 {
     cudaError_t e = prepare_device_kernels();
     if (e != cudaSuccess) return e;
+    if (!forward_layers_ok(arith, layers)) return cudaErrorInvalidValue;
     if (n_items <= 0 || total_units == 0) return cudaSuccess;
     ctas = std::max(1u, std::min(ctas, total_units));
     if (arith == kFast) k_forward_batched<kFast><<<ctas, NT, kFwdSmem, s>>>(items, n_items, total_units, ticket);
+    else if (layers == FwdTall::by)
+        k_forward_batched<kStrict, FwdTall><<<ctas, FwdTall::nt, FwdTall::smem, s>>>(items, n_items, total_units,
+                                                                                     ticket);
     else k_forward_batched<kStrict><<<ctas, NT, kFwdSmem, s>>>(items, n_items, total_units, ticket);
     return cudaGetLastError();
 }
