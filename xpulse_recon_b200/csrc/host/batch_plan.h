@@ -15,12 +15,10 @@ namespace xpr {
 inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 inline size_t dtype_size(int dt) { return dt == XPR_F32 ? 4 : 2; }
 inline uint32_t entries_of(const xpr_batch_problem &p) { return p.per_subset * (p.modules ? p.modules : 1u); }
-// entries per forward work unit for `splits` runs of equal length (a run need not be a
-// whole number of metadata groups: the last group of a run marks its missing entries
-// skipped)
+// entries per forward work unit (a multiple of the metadata group of 4) for `splits` runs
 inline uint32_t per_split_for(uint32_t entries, int splits)
 {
-    return (uint32_t)div_up(entries, (uint64_t)(splits > 1 ? splits : 1));
+    return (uint32_t)div_up(div_up(entries, (uint64_t)(splits > 1 ? splits : 1)), 4) * 4;
 }
 
 struct PlannedProblem {
