@@ -88,14 +88,14 @@ NOMINAL_FP32_LANES = 148 * 128
 # c2 geometry's central 256-layer slab (150,994,944 voxels, FP32 storage); scaled to a
 # launch by its voxel count for the same geometry
 MEASURED_TRAFFIC_PER_VOXEL = {
-    "strict": {"forward": 715.2e6 / 150994944, "backward": 1211.8e6 / 150994944},
+    "strict": {"forward": 716.4e6 / 150994944, "backward": 1211.8e6 / 150994944},
     "fast": {"forward": 716.1e6 / 150994944, "backward": 1219.0e6 / 150994944},
 }
 # executed-work figures of the same captures (profiles/k_*_c2slab.md): issue-active share,
 # l1tex (shared-memory pipe) throughput and thread instructions per (voxel, projection) pair
 MEASURED_PROFILE = {
-    "strict": {"forward": {"issue_active_pct": 71.7, "l1tex_pct": 73.7, "fma_pipe_pct": 52.4,
-                           "thread_inst_per_pair": 16.5, "shared_atomic_replay_pct": 48.9},
+    "strict": {"forward": {"issue_active_pct": 67.7, "l1tex_pct": 74.5, "fma_pipe_pct": 56.2,
+                           "thread_inst_per_pair": 14.5, "shared_atomic_replay_pct": 48.6},
                "backward": {"issue_active_pct": 70.7, "l1tex_pct": 46.7, "fma_pipe_pct": 65.8,
                             "thread_inst_per_pair": 15.7},
                "source": "ncu --set full, c2 geometry 256-layer slab: profiles/k_forward_tiled_strict_c2slab.md, "
