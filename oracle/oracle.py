@@ -1,7 +1,8 @@
 """ctypes front end of the CPU oracle (test infrastructure only).
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
-this module, and only as the checker.  It wraps:
+this module, and only to compare the product's results with, or (the CPU baseline) to
+time the reference's kernels on the host.  It wraps:
 
 * ``libxpr_oracle.so`` -- the C restatement of the reference path (xpr_oracle.c);
 * ``libxpr_ref.so``    -- the reference's own OpenCL kernels compiled for the CPU

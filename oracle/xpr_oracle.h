@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product links this library: it is
  * loaded by tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline
- * leg, and only as the checker.  It restates, in plain C, the algorithm of
+ * leg, and only to compare the product's results with.  It restates, in plain C, the algorithm of
  * ebarjou/xpulse_recon ("XPRecon") for this path:
  *
  *   - geometry -> ProjData          src/reconstruction/dataset/geometry.hpp:35-76,182-328

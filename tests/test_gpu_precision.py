@@ -1,10 +1,11 @@
 """Precision of the reduced-storage forms against the FP64 oracle.
 
-Whole naive reconstructions through the drop-in host entry point (FAST contract,
+Whole naive reconstructions through the drop-in host entry point (STRICT contract,
 geometry matrices built in double, detector images and ratios stored in FP32, BF16 or
 FP16 with FP32 accumulation and an FP32 volume) are compared with the same algorithm
 run in double precision on the CPU (oracle/xpr_oracle.c, orc64_recon_naive), on
-projections of a seeded ellipsoid phantom with Poisson noise.
+projections of a seeded ellipsoid phantom with Poisson noise (simulated with the FAST
+forward projector).
 
 Measure: relative RMSE = ||v - v64||_2 / ||v64||_2 over the measurement region: the
 voxels finite in both inside the grid's inscribed cylinder, without the two layers at
@@ -16,7 +17,7 @@ are NaN in both, by the algorithm's 0/0.
 
 Storage forms (ratio / measured images): fp32, fp16, bf16 = BF16 ratio with FP16
 images, bf16_fp32img = BF16 ratio with FP32 images, bf16_all = BF16 ratio and BF16
-images.  Tolerance (written here): 1e-3 relative RMSE, the north star's bound, which
+images.  Tolerance (written here): 1e-3 relative RMSE, the precision target, which
 FP32 and FP16 storage meet (measured 5.5e-4 - 7.6e-4 on B200).  Every BF16 form is a
 known miss, kept as a strict xfail so that the miss stays visible: a BF16 ratio alone
 gives 1.1e-3 - 1.4e-3 (its 2^-9 relative rounding of the log-ratio, largest in the
